@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark of the neighbor-search hot path (one JSON line on rank 0).
+
+Default workload (--workload knn_multicloud_4096): 4,096 independent clouds, sizes
+log-uniform in [512, 65536] (about 5.5e7 points), each a 1-8 component Gaussian
+mixture normalised to the unit cube; queries = each cloud's own points; KNN K = 32,
+r = 0.2. One step = grid build + learned-partition search of every cloud, replayed from
+one CUDA graph (rtnn_plan_execute), inputs resident in HBM (0.66 GB of points, larger
+than the 126 MB L2, so no flush is needed between steps). The same data searched by the
+plain grid (no partition) is timed in the same run and reported as `plain_value`.
+
+`e2e` is the same metric through the public C ABI with host (pinned) buffers:
+rtnn_search_batched with the point upload and the result download inside the timed region.
+`cpu_baseline` / `--impl reference`: the reference's own CPU path for this search,
+check.cpp's brute-force KNN (compiled from the reference sources into oracle/_ref/refcheck),
+timed on a bounded sample of clouds with one process per host core.
+
+Multi-GPU (torchrun): every rank searches its own instance of the workload (seeds offset
+by rank; weak scaling, no collective in the data path); value = all queries / max rank time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="rtnn", choices=["rtnn", "reference"])
+    ap.add_argument("--workload", default="knn_multicloud_4096",
+                    choices=["knn_multicloud_4096", "knn_surface_1e7", "knn_gmm_1e6",
+                             "radius_uniform_1e5", "sph_lattice_5e7"])
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink point counts (tests)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+def make_workload(name, scale, rank):
+    from rtnn_b200 import workloads as wl
+    cfg = dict(wl.CONFIGS[name])
+    s = 1000 * rank
+    if name == "knn_multicloud_4096":
+        p, off = wl.multicloud(seed=3 + s, scale=scale)
+        cfg.update(points=p, offsets=off, queries=None, qoffsets=None)
+    elif name == "knn_surface_1e7":
+        p = wl.surfaces(seed=2 + s, scale=scale)
+        cfg.update(points=p, offsets=np.array([0, len(p)], np.uint64), queries=None, qoffsets=None)
+    elif name == "knn_gmm_1e6":
+        p, q = wl.gmm(seed=1 + s, scale=scale)
+        cfg.update(points=p, offsets=np.array([0, len(p)], np.uint64), queries=q,
+                   qoffsets=np.array([0, len(q)], np.uint64))
+    elif name == "radius_uniform_1e5":
+        p = wl.uniform_cube(seed=0 + s, scale=scale)
+        cfg.update(points=p, offsets=np.array([0, len(p)], np.uint64), queries=None, qoffsets=None)
+    else:
+        p = wl.sph_step(wl.sph_lattice(seed=4 + s, scale=scale), seed=5 + s)
+        cfg.update(points=p, offsets=np.array([0, len(p)], np.uint64), queries=None, qoffsets=None)
+    cfg["n_queries"] = int(len(p) if cfg["queries"] is None else len(cfg["queries"]))
+    cfg["name"] = name
+    return cfg
+
+
+def training_clouds(name, scale, rank):
+    """Clouds of other seeds (never the measured one) for the width model."""
+    from rtnn_b200 import workloads as wl
+    s = 1000 * rank + 100
+    out = []
+    if name == "knn_multicloud_4096":
+        p, off = wl.multicloud(n_clouds=96, seed=s + 7)
+        for c in range(len(off) - 1):
+            out.append((p[int(off[c]):int(off[c + 1])], None))
+    elif name == "knn_surface_1e7":
+        for i in range(20):
+            out.append((wl.surfaces(seed=s + i, scale=0.05 * max(scale, 0.02)), None))
+    elif name == "knn_gmm_1e6":
+        for i in range(4):
+            out.append(wl.gmm(seed=s + i, scale=0.25 * scale))
+    elif name == "radius_uniform_1e5":
+        for i in range(4):
+            out.append((wl.uniform_cube(seed=s + i, scale=scale), None))
+    else:
+        for i in range(2):
+            out.append((wl.sph_lattice(seed=s + i, scale=0.02 * scale), None))
+    return out
+
+
+def train_model(ctx, cfg, scale, rank):
+    import torch
+    feats, tgts = [], []
+    for p, q in training_clouds(cfg["name"], scale, rank):
+        tp = torch.from_numpy(np.ascontiguousarray(p)).cuda()
+        tq = None if q is None else torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        f, t = ctx.collect_training(tp, tq, cfg["mode"], cfg["radius"], cfg["k"])
+        feats.append(f)
+        tgts.append(t)
+    f = torch.cat(feats)
+    t = torch.cat(tgts)
+    perm = torch.randperm(f.shape[0], device=f.device, generator=torch.Generator(device=f.device).manual_seed(0))
+    f = f[perm].contiguous()
+    t = t[perm].contiguous()
+    losses = ctx.train_model(f, t, epochs=8, batch=16384, lr=3e-3, seed=rank)
+    return {"samples": int(f.shape[0]), "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+
+
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+def cpu_reference_sample(cfg, seconds, threads, seed=0):
+    """The reference's CPU search on a bounded sample: check.cpp's brute-force KNN
+    (oracle/_ref/refcheck, one process per core over disjoint query ranges) for KNN
+    workloads; radius mode has no CPU search in the reference (sanityCheckRadius only
+    validates rows), so the oracle's restatement of that brute force stands in."""
+    import oracle
+    p, off = cfg["points"], cfg["offsets"]
+    q, qoff = cfg["queries"], cfg["qoffsets"]
+    if qoff is None:
+        qoff = off
+    rng = np.random.default_rng(seed)
+    n_clouds = len(off) - 1
+    use_ref = cfg["mode"] == "knn" and oracle.ref_available()
+    done_q, elapsed = 0, 0.0
+    order = rng.permutation(n_clouds)
+    for c in order:
+        cp = p[int(off[c]):int(off[c + 1])]
+        cq = cp if q is None else q[int(qoff[c]):int(qoff[c + 1])]
+        if len(cq) == 0 or len(cp) == 0:
+            continue
+        # bound the per-cloud sample: at most ~2e9 distance tests
+        nq = int(min(len(cq), max(64, 2e9 // max(len(cp), 1))))
+        sel = np.sort(rng.choice(len(cq), nq, replace=False)) if nq < len(cq) else np.arange(len(cq))
+        qs = np.ascontiguousarray(cq[sel])
+        if use_ref:
+            rows = oracle.grid_search(cp, qs, cfg["mode"], cfg["radius"], cfg["k"], threads)
+            with tempfile.TemporaryDirectory() as d:
+                pf, qf, rf = (os.path.join(d, n) for n in ("p.bin", "q.bin", "r.bin"))
+                cp.astype(np.float32).tofile(pf)
+                qs.astype(np.float32).tofile(qf)
+                rows.tofile(rf)
+                exe = os.path.join(oracle.REF_DIR, "refcheck")
+                bounds = np.linspace(0, nq, threads + 1).astype(int)
+                t0 = time.perf_counter()
+                procs = [subprocess.Popen([exe, pf, qf, rf, "knn", repr(float(cfg["radius"])),
+                                           str(cfg["k"]), str(bounds[i]), str(bounds[i + 1])],
+                                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                         for i in range(threads) if bounds[i + 1] > bounds[i]]
+                rcs = [pp.wait() for pp in procs]
+                elapsed += time.perf_counter() - t0
+                if any(rcs):
+                    raise RuntimeError("reference check rejected the oracle rows")
+        else:
+            t0 = time.perf_counter()
+            oracle.bruteforce(cp, qs, cfg["mode"], cfg["radius"], cfg["k"], threads)
+            elapsed += time.perf_counter() - t0
+        done_q += nq
+        if elapsed >= seconds:
+            break
+    return {"value": done_q / max(elapsed, 1e-9), "unit": "queries/s", "cores": threads,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"{done_q} queries of the workload, brute force over their own cloud "
+                      f"({'check.cpp sanityCheckKNN via oracle/_ref/refcheck' if use_ref else 'oracle restatement of check.cpp:34-48'}), "
+                      f"{elapsed:.1f} s on {threads} host threads"}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+# ---------------------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cfg = make_workload(args.workload, args.scale, 0)
+    threads = os.cpu_count() or 1
+    vals = []
+    per_step = max(2.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_sample(cfg, per_step, threads, seed=i)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median([r["value"] for r in vals])
+    line = {"impl": "reference", "metric": "queries/s", "value": v, "unit": "queries/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
+            "config": {"workload": args.workload, "mode": cfg["mode"], "radius": cfg["radius"],
+                       "k": cfg["k"], "n_points": int(len(cfg["points"])),
+                       "n_queries": cfg["n_queries"], "n_clouds": int(len(cfg["offsets"]) - 1)},
+            "cpu_baseline": {**vals[-1], "value": v},
+            "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_rtnn(args, rank, world):
+    import torch
+    import rtnn_b200
+    from rtnn_b200 import build as rb
+    rb.build()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    cfg = make_workload(args.workload, args.scale, rank)
+    ctx = rtnn_b200.Context(dev)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    model_info = train_model(ctx, cfg, args.scale, rank)
+
+    tp = torch.from_numpy(cfg["points"]).cuda()
+    tq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).cuda()
+    Q, K = cfg["n_queries"], cfg["k"]
+    out = torch.empty((Q, K), dtype=torch.int32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(plan, steps, warmup, clocks=None):
+        for _ in range(warmup):
+            plan.execute(tp, tq, out)
+        barrier()
+        if clocks:
+            clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            plan.execute(tp, tq, out)
+        e1.record(stream)
+        barrier()
+        ck = clocks.stop() if clocks else None
+        return max_over_ranks(e0.elapsed_time(e1) / steps), ck
+
+    common = dict(mode=cfg["mode"], radius=cfg["radius"], k=K)
+    learned = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=True, **common)
+    ms_learned, clocks = timed(learned, args.steps, args.warmup, ClockSampler(dev))
+    st = rtnn_b200.Stats()
+    learned.execute(tp, tq, out, stats=st)
+    launches_per_step = st.n_launches
+    fallback = st.n_fallback
+    result_learned = out.clone()
+    learned.close()
+
+    plain_ms = None
+    if not args.no_plain:
+        plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
+        plain_ms, _ = timed(plain, args.steps, max(1, args.warmup // 2))
+        plain.execute(tp, tq, out)
+        identical = bool(torch.equal(_row_sets(out), _row_sets(result_learned)))
+        plain.close()
+    else:
+        identical = None
+
+    # dominant kernel (search, both passes) timed with the library's events on `stream`
+    nog = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=False, **common)
+    ms_search, ms_build, ms_part = [], [], []
+    for _ in range(max(3, args.steps)):
+        s2 = rtnn_b200.Stats()
+        nog.execute(tp, tq, out, stats=s2)
+        ms_search.append(s2.ms_search)
+        ms_build.append(s2.ms_build)
+        ms_part.append(s2.ms_partition)
+    nog.close()
+    ms_s = statistics.mean(ms_search)
+    N = int(len(cfg["points"]))
+    alg_bytes = 16 * Q + 16 * N + 4 * Q * K    # sorted queries + sorted points read once, rows written
+    pk, pk_src = peaks()
+    achieved = alg_bytes / (ms_s * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
+                "traffic": None, "kernel": "k_search (both passes)", "peak_source": pk_src,
+                "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": round(ms_s, 4)}
+
+    e2e = None
+    if not args.no_e2e:
+        hp = torch.from_numpy(cfg["points"]).pin_memory()
+        hq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).pin_memory()
+        ho = torch.empty((Q, K), dtype=torch.int32).pin_memory()
+        hp_np, ho_np = hp.numpy(), ho.numpy()
+        hq_np = None if hq is None else hq.numpy()
+        ctx.search_batched(hp_np, cfg["offsets"], hq_np, cfg["qoffsets"], learned=True, out=ho_np, **common)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.search_batched(hp_np, cfg["offsets"], hq_np, cfg["qoffsets"], learned=True, out=ho_np, **common)
+        dt = max_over_ranks((time.perf_counter() - t0) / args.steps)
+        h2d = 12 * N + (0 if hq is None else 12 * Q)
+        e2e = {"value": world * Q / dt, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 4 * Q * K, "ms_per_step": round(dt * 1e3, 3)}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_reference_sample(cfg, args.cpu_seconds, os.cpu_count() or 1)
+
+    value = world * Q / (ms_learned * 1e-3)
+    line = {"metric": "queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_learned, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded numpy PCG64)",
+            "config": {"workload": args.workload, "mode": cfg["mode"], "radius": cfg["radius"],
+                       "k": K, "n_points": N, "n_queries": Q,
+                       "n_clouds": int(len(cfg["offsets"]) - 1),
+                       "path": "learned partition + batched persistent search, CUDA graph",
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "plain_value": None if plain_ms is None else world * Q / (plain_ms * 1e-3),
+            "learned_over_plain": None if plain_ms is None else plain_ms / ms_learned,
+            "identical_sets": identical, "fallback_queries": int(fallback),
+            "stage_ms": {"build": round(statistics.mean(ms_build), 3),
+                         "partition": round(statistics.mean(ms_part), 3), "search": round(ms_s, 3)},
+            "model": model_info, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches_per_step * args.steps), "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _row_sets(t):
+    """Rows with entries sorted (set comparison on the GPU)."""
+    import torch
+    big = torch.iinfo(torch.int32).max
+    s, _ = torch.sort(torch.where(t < 0, torch.full_like(t, big), t), dim=1)
+    return s
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_rtnn(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

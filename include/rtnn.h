@@ -1,0 +1,161 @@
+/*
+ * rtnn.h -- C ABI of the B200-native neighbor-search engine (librtnn_b200.so).
+ *
+ * The reference (horizon-research/rtnn) has no library API: its boundary is the
+ * `optixNSearch` executable (src/optixNSearch/main.cpp:47-161). Each entry point
+ * below replaces one step of that executable; the replaced reference code is cited
+ * beside it. All calls return an rtnn_status and never throw across the ABI; the
+ * message of the last failure on a context is available from rtnn_last_error().
+ *
+ * Output contract (src/optixNSearch/search.cpp:18, geometry.cu:72-83,
+ * camera.cu:99-104): a row-major Q x K int32 buffer, row q holding the neighbors of
+ * query q; unused slots hold -1 (the reference's UINT_MAX). Indices refer to the
+ * caller's point order (the reference returns indices into its Morton-sorted copy).
+ *
+ * Predicates (distance d = ((dx*dx + dy*dy) + dz*dz) in FP32, each operation
+ * rounded, no FMA: src/sutil/vec_math.h:527-530, check.cpp:36-37):
+ *   RTNN_MODE_RADIUS: d < r*r, the query itself included (geometry.cu:61-66).
+ *   RTNN_MODE_KNN:    0 < d < r*r, coincident points excluded (geometry.cu:187).
+ * When more than K points qualify, the K smallest by (d, index) are returned, so the
+ * neighbor set of every row is deterministic and exact.
+ *
+ * Threading: a context is not thread-safe; use one context per host thread. Calls on
+ * a context are ordered on the context's CUDA stream.
+ */
+#ifndef RTNN_H_
+#define RTNN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rtnn_status {
+  RTNN_OK = 0,
+  RTNN_ERR_INVALID_ARGUMENT = 1,  /* bad pointer, size, radius or flag combination */
+  RTNN_ERR_CUDA = 2,              /* a CUDA runtime call failed */
+  RTNN_ERR_OUT_OF_MEMORY = 3,     /* device allocation failed */
+  RTNN_ERR_UNSUPPORTED_K = 4,     /* K == 0 or K > RTNN_MAX_K */
+  RTNN_ERR_DEVICE_TIMEOUT = 5,    /* a bounded device-side wait gave up */
+  RTNN_ERR_NO_DEVICE = 6,         /* no CUDA device, or the device id is out of range */
+  RTNN_ERR_NO_MODEL = 7,          /* RTNN_FLAG_LEARNED without a loaded width model */
+  RTNN_ERR_INTERNAL = 8           /* a device-side consistency check failed */
+} rtnn_status;
+
+typedef enum rtnn_mode {
+  RTNN_MODE_RADIUS = 0,           /* -sm radius (util.cpp:220-227) */
+  RTNN_MODE_KNN = 1               /* -sm knn */
+} rtnn_mode;
+
+/* Largest K any search accepts (the reference bakes K in at compile time,
+ * src/optixNSearch/CMakeLists.txt:58-61; here it is a run-time argument up to this). */
+#define RTNN_MAX_K 128u
+
+/* Flags for rtnn_search / rtnn_search_batched / rtnn_plan_create. */
+#define RTNN_FLAG_DEVICE_POINTERS 0x1u  /* points, queries and out are device pointers */
+#define RTNN_FLAG_PARTITION       0x2u  /* density buckets with analytic widths + exact fallback
+                                           (replaces the query partitioning of sort.cpp:393-498) */
+#define RTNN_FLAG_LEARNED         0x4u  /* density buckets with widths from the loaded MLP + exact
+                                           fallback (replaces the analytic heuristic) */
+#define RTNN_FLAG_SORTED_ROWS     0x8u  /* sort each output row by (distance, index) */
+#define RTNN_FLAG_LOCAL_INDICES   0x10u /* batched: indices relative to the point's own cloud */
+
+/* Per-call statistics (all optional to read). Times are device times measured with
+ * CUDA events on the context stream (graph replays report ms_total only). */
+typedef struct rtnn_stats {
+  uint64_t n_points;
+  uint64_t n_queries;
+  uint32_t n_clouds;
+  uint32_t n_buckets;        /* distinct width levels used by the partition (1 when plain) */
+  uint64_t n_fallback;       /* queries re-searched at the full radius */
+  uint64_t n_tiles;          /* 32-query work items of the first search pass */
+  uint64_t n_cells;          /* total grid cells over all clouds */
+  float cell_size;           /* cell edge of the first cloud */
+  uint32_t grid_dims[3];     /* grid dimensions of the first cloud */
+  float ms_build;            /* bounds + grid build + query ordering */
+  float ms_partition;        /* per-query widths (analytic or learned) */
+  float ms_search;           /* both search passes and the output write */
+  float ms_total;            /* device time of the whole call (copies excluded) */
+  uint32_t n_launches;       /* kernels of this library launched by the call */
+  uint32_t pad;
+} rtnn_stats;
+
+typedef struct rtnn_ctx rtnn_ctx;
+typedef struct rtnn_plan rtnn_plan;
+
+/* Creates a context on CUDA device `device` (replaces setDevice, main.cpp:9-24).
+ * The context owns one CUDA stream and a grow-only cache of device buffers. */
+rtnn_status rtnn_create(rtnn_ctx** ctx, int device);
+
+/* Frees every device buffer of the context (replaces cleanupState, optix.cpp:628-677). */
+rtnn_status rtnn_destroy(rtnn_ctx* ctx);
+
+/* Message of the last failed call on this context ("" when none). */
+const char* rtnn_last_error(const rtnn_ctx* ctx);
+
+/* Makes the context issue its work on `stream` (a cudaStream_t); NULL restores the
+ * context's own stream. */
+rtnn_status rtnn_set_stream(rtnn_ctx* ctx, void* stream);
+
+/* Returns 1 when `k` is accepted by the searches, else 0. */
+int rtnn_k_supported(uint32_t k);
+
+/* Version string of the library. */
+const char* rtnn_version(void);
+
+/* One fixed-radius or KNN search of `n_queries` queries against `n_points` points.
+ * Replaces the whole timed region of optixNSearch (main.cpp:91-148: sortParticles,
+ * createGeometry, gasSortSearch, search) for `-f points -q queries -sm mode -r radius
+ * -k k`. `queries` may be NULL: the points are then also the queries (util.cpp:371).
+ * points/queries: xyz float triples (12 bytes each, AoS as read by util.cpp:101-135).
+ * out: n_queries * k int32. Host pointers unless RTNN_FLAG_DEVICE_POINTERS. */
+rtnn_status rtnn_search(rtnn_ctx* ctx,
+                        const float* points, uint64_t n_points,
+                        const float* queries, uint64_t n_queries,
+                        rtnn_mode mode, float radius, uint32_t k, uint32_t flags,
+                        int32_t* out, rtnn_stats* stats);
+
+/* Many independent point clouds searched in one persistent launch (no counterpart in
+ * the reference, which searches one cloud per process). Cloud c owns points
+ * [point_offsets[c], point_offsets[c+1]) and queries [query_offsets[c],
+ * query_offsets[c+1]); queries == NULL means every cloud's points are its queries.
+ * point_offsets / query_offsets are HOST arrays of n_clouds + 1 entries. Row q of out
+ * holds neighbors of query q from the query's own cloud only. */
+rtnn_status rtnn_search_batched(rtnn_ctx* ctx,
+                                const float* points, const uint64_t* point_offsets,
+                                uint32_t n_clouds,
+                                const float* queries, const uint64_t* query_offsets,
+                                rtnn_mode mode, float radius, uint32_t k, uint32_t flags,
+                                int32_t* out, rtnn_stats* stats);
+
+/* A plan fixes the shapes of a (batched) search so that grid build and search can be
+ * captured once in a CUDA graph and replayed on new point data of the same shape.
+ * Device pointers only. use_graph = 0 issues the kernels directly on every execute. */
+rtnn_status rtnn_plan_create(rtnn_ctx* ctx, rtnn_plan** plan,
+                             const uint64_t* point_offsets, uint32_t n_clouds,
+                             const uint64_t* query_offsets, /* NULL: queries are points */
+                             rtnn_mode mode, float radius, uint32_t k, uint32_t flags,
+                             int use_graph);
+rtnn_status rtnn_plan_execute(rtnn_plan* plan, const float* d_points, const float* d_queries,
+                              int32_t* d_out, rtnn_stats* stats);
+rtnn_status rtnn_plan_destroy(rtnn_plan* plan);
+
+/* Search-tuning knobs chosen by the autotuner (rtnn_b200/autotune.py caches them). */
+typedef struct rtnn_tuning {
+  float cell_ratio;      /* cell edge = radius * cell_ratio (reference: 1/crRatio, sort.cpp:80) */
+  float cell_budget;     /* max grid cells per point before the cell edge is grown */
+  uint32_t warps_per_block;   /* search kernel block size in warps */
+  uint32_t blocks_per_sm;     /* persistent search grid = SMs * blocks_per_sm */
+  float width_margin;    /* learned width = margin * predicted K-th distance */
+} rtnn_tuning;
+
+rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);
+rtnn_status rtnn_set_tuning(rtnn_ctx* ctx, const rtnn_tuning* tuning);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTNN_H_ */

@@ -1,0 +1,863 @@
+// api.cu -- C ABI (include/rtnn.h) and the host-side pipeline driver.
+//
+// The pipeline replaces the timed region of optixNSearch (src/optixNSearch/main.cpp:91-148):
+//   uploadData/computeMinMax (optix.cpp:117-168)      -> k_bbox, k_grid_plan
+//   sortParticles/gridSort (sort.cpp:500-692)         -> k_count, scan, k_scatter
+//   query Morton order + partition (sort.cpp:393-498) -> k_query_keys, radix sort, k_widths
+//   createGeometry/gasSortSearch/search (search.cpp)  -> k_search (+ fallback pass)
+// Every step is issued on one stream with no host synchronisation, so the same code
+// path is captured into a CUDA graph by rtnn_plan_execute. Sizes that are only known on
+// the device (cells per cloud, fallback count) are read by the kernels themselves.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rtnn.h"
+#include "../../include/rtnn_learn.h"
+#include "kernels.h"
+
+using namespace rtnn;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+  if (bytes < 16) bytes = 16;
+  if (b.cap >= bytes) return cudaSuccess;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  const size_t want = bytes + bytes / 8;
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); b.p = nullptr; return e; }
+    b.cap = bytes;
+    return cudaSuccess;
+  }
+  b.cap = want;
+  return cudaSuccess;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+struct Workspace {
+  DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth, fbpos,
+      fbcloud, hist, scan_state, counters, in_pts, in_qs, out, feats, cellsz, kth;
+  void release_all() {
+    for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
+                      &vals1, &sq, &qwidth, &fbpos, &fbcloud, &hist, &scan_state, &counters,
+                      &in_pts, &in_qs, &out, &feats, &cellsz, &kth})
+      release(*b);
+  }
+};
+
+struct Shapes {
+  uint32_t n_clouds = 1;
+  uint64_t N = 0, Q = 0;
+  bool single = true;
+  std::vector<uint32_t> tab;  // batched: point_off | query_off | chunk_base | qchunk_base | tile_base
+  uint32_t n_chunks = 0, n_qchunks = 0, n_tiles = 0;
+  uint64_t max_cloud_q = 0;
+  uint32_t morton_bits = 1, key_bits = 8;
+  bool key64 = false;
+  float cell_budget = 8.f;
+  uint64_t cell_capacity = 0;
+};
+
+struct Params {
+  rtnn_mode mode;
+  float radius;
+  uint32_t k;
+  uint32_t flags;
+};
+
+uint32_t ceil_log2(uint64_t x) {
+  uint32_t b = 0;
+  while ((1ull << b) < x) ++b;
+  return b;
+}
+
+}  // namespace
+
+struct rtnn_ctx {
+  int device = 0;
+  int n_sms = 148;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  rtnn_tuning tuning{0.5f, 16.f, 4u, 0u, 1.25f};
+  Workspace ws;
+  cudaEvent_t ev[6] = {};
+  Counters* h_ctr = nullptr;   // pinned
+  CloudGrid* h_grid = nullptr; // pinned
+  DevBuf model;
+  bool has_model = false;
+  DevBuf train_grad, train_m, train_v, train_loss;
+};
+
+struct rtnn_plan {
+  rtnn_ctx* ctx = nullptr;
+  Shapes sh;
+  Params pr{};
+  Workspace ws;
+  bool use_graph = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const float* g_pts = nullptr;
+  const float* g_qs = nullptr;
+  int32_t* g_out = nullptr;
+};
+
+namespace {
+
+rtnn_status fail(rtnn_ctx* c, rtnn_status st, const std::string& msg) {
+  if (c) c->err = msg;
+  return st;
+}
+
+rtnn_status cuda_fail(rtnn_ctx* c, cudaError_t e, const char* where) {
+  const rtnn_status st = (e == cudaErrorMemoryAllocation) ? RTNN_ERR_OUT_OF_MEMORY : RTNN_ERR_CUDA;
+  return fail(c, st, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define RTNN_CU(call, where)                                   \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, where);     \
+  } while (0)
+
+rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32_t k,
+                       uint32_t flags) {
+  if (!(std::isfinite(radius) && radius >= 1e-30f))
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "radius must be a finite number > 0");
+  if (!rtnn_k_supported(k))
+    return fail(c, RTNN_ERR_UNSUPPORTED_K, "k must be in [1, " + std::to_string(RTNN_MAX_K) + "]");
+  if (N >= (1ull << 31) || Q >= (1ull << 31))
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 points and queries");
+  const uint32_t known = RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED |
+                         RTNN_FLAG_SORTED_ROWS | RTNN_FLAG_LOCAL_INDICES;
+  if (flags & ~known) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "unknown flag bits");
+  if ((flags & RTNN_FLAG_LEARNED) && !c->has_model)
+    return fail(c, RTNN_ERR_NO_MODEL, "RTNN_FLAG_LEARNED needs a width model (rtnn_model_set or rtnn_model_train)");
+  return RTNN_OK;
+}
+
+void finish_shapes(Shapes& sh, const rtnn_tuning& tu) {
+  uint32_t mb = (ceil_log2(std::max<uint64_t>(sh.max_cloud_q, 2)) + 2) / 3;
+  mb = std::max(1u, std::min(10u, mb));
+  const uint32_t cb = ceil_log2(sh.n_clouds);
+  if (cb + 3 * mb > 64) mb = (64 - cb) / 3;
+  sh.morton_bits = mb;
+  sh.key_bits = std::max(8u, cb + 3 * mb);
+  sh.key64 = sh.key_bits > 32;
+  // cells: each cloud gets max(64, budget * points); indices stay 32-bit
+  double budget = std::max(0.01f, tu.cell_budget);
+  const double limit = 4.0e9;
+  if (budget * (double)sh.N + 64.0 * sh.n_clouds > limit)
+    budget = std::max(0.01, (limit - 64.0 * sh.n_clouds) / std::max<double>(1.0, (double)sh.N));
+  sh.cell_budget = (float)budget;
+  sh.cell_capacity = (uint64_t)std::ceil(budget * (double)sh.N) + 64ull * sh.n_clouds + 64;
+}
+
+Shapes single_shapes(uint64_t N, uint64_t Q, const rtnn_tuning& tu) {
+  Shapes sh;
+  sh.n_clouds = 1;
+  sh.N = N;
+  sh.Q = Q;
+  sh.single = true;
+  sh.n_chunks = (uint32_t)((N + kChunk - 1) / kChunk);
+  sh.n_qchunks = (uint32_t)((Q + kChunk - 1) / kChunk);
+  sh.n_tiles = (uint32_t)((Q + kTile - 1) / kTile);
+  sh.max_cloud_q = Q;
+  finish_shapes(sh, tu);
+  return sh;
+}
+
+rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_clouds,
+                           const uint64_t* query_off, const rtnn_tuning& tu, Shapes& sh) {
+  if (n_clouds == 0) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "n_clouds must be > 0");
+  if (!point_off) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "point_offsets is NULL");
+  const uint64_t* qoff = query_off ? query_off : point_off;
+  if (point_off[0] != 0 || qoff[0] != 0)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "offsets must start at 0");
+  const uint32_t n1 = n_clouds + 1;
+  sh.n_clouds = n_clouds;
+  sh.single = false;
+  sh.tab.assign(5ull * n1, 0u);
+  uint32_t* po = sh.tab.data();
+  uint32_t* qo = po + n1;
+  uint32_t* cb = qo + n1;
+  uint32_t* qb = cb + n1;
+  uint32_t* tb = qb + n1;
+  uint64_t chunks = 0, qchunks = 0, tiles = 0, maxq = 0;
+  for (uint32_t i = 0; i < n_clouds; ++i) {
+    if (point_off[i + 1] < point_off[i] || qoff[i + 1] < qoff[i])
+      return fail(c, RTNN_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
+    const uint64_t np = point_off[i + 1] - point_off[i], nq = qoff[i + 1] - qoff[i];
+    po[i] = (uint32_t)point_off[i];
+    qo[i] = (uint32_t)qoff[i];
+    cb[i] = (uint32_t)chunks;
+    qb[i] = (uint32_t)qchunks;
+    tb[i] = (uint32_t)tiles;
+    chunks += (np + kChunk - 1) / kChunk;
+    qchunks += (nq + kChunk - 1) / kChunk;
+    tiles += (nq + kTile - 1) / kTile;
+    maxq = std::max(maxq, nq);
+  }
+  sh.N = point_off[n_clouds];
+  sh.Q = qoff[n_clouds];
+  if (sh.N >= (1ull << 31) || sh.Q >= (1ull << 31))
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 points and queries");
+  po[n_clouds] = (uint32_t)sh.N;
+  qo[n_clouds] = (uint32_t)sh.Q;
+  cb[n_clouds] = (uint32_t)chunks;
+  qb[n_clouds] = (uint32_t)qchunks;
+  tb[n_clouds] = (uint32_t)tiles;
+  sh.n_chunks = (uint32_t)chunks;
+  sh.n_qchunks = (uint32_t)qchunks;
+  sh.n_tiles = (uint32_t)tiles;
+  sh.max_cloud_q = maxq;
+  finish_shapes(sh, tu);
+  return RTNN_OK;
+}
+
+bool partitioned(const Params& p) { return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0; }
+
+rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr) {
+  const uint64_t n1 = sh.n_clouds + 1ull;
+  const uint64_t N = std::max<uint64_t>(sh.N, 1), Q = std::max<uint64_t>(sh.Q, 1);
+  const uint64_t rt = radix_tiles_for(Q);
+  const uint64_t scan_n = std::max<uint64_t>(sh.cell_capacity + 1, 256ull * rt);
+  RTNN_CU(ensure(ws.tables, 5 * n1 * 4), "alloc tables");
+  RTNN_CU(ensure(ws.grids, sh.n_clouds * sizeof(CloudGrid)), "alloc grids");
+  RTNN_CU(ensure(ws.bbox, 6ull * sh.n_clouds * 4), "alloc bbox");
+  RTNN_CU(ensure(ws.cells, (sh.cell_capacity + 1) * 4), "alloc cells");
+  RTNN_CU(ensure(ws.rank, N * 4), "alloc rank");
+  RTNN_CU(ensure(ws.spts, N * 16), "alloc sorted points");
+  RTNN_CU(ensure(ws.keys0, Q * (sh.key64 ? 8 : 4)), "alloc keys");
+  RTNN_CU(ensure(ws.keys1, Q * (sh.key64 ? 8 : 4)), "alloc keys");
+  RTNN_CU(ensure(ws.vals0, Q * 4), "alloc vals");
+  RTNN_CU(ensure(ws.vals1, Q * 4), "alloc vals");
+  RTNN_CU(ensure(ws.sq, Q * 16), "alloc sorted queries");
+  if (partitioned(pr)) {
+    RTNN_CU(ensure(ws.qwidth, Q * 4), "alloc widths");
+    RTNN_CU(ensure(ws.fbpos, Q * 4), "alloc fallback list");
+    RTNN_CU(ensure(ws.fbcloud, Q * 4), "alloc fallback list");
+  }
+  RTNN_CU(ensure(ws.hist, 256 * rt * 4), "alloc radix histogram");
+  RTNN_CU(ensure(ws.scan_state, scan_tiles_for(scan_n) * 8), "alloc scan state");
+  RTNN_CU(ensure(ws.counters, sizeof(Counters)), "alloc counters");
+  return RTNN_OK;
+}
+
+CloudTables tables_of(const Workspace& ws, uint32_t n_clouds) {
+  const uint32_t* t = (const uint32_t*)ws.tables.p;
+  const uint32_t n1 = n_clouds + 1;
+  CloudTables ct;
+  ct.point_off = t;
+  ct.query_off = t + n1;
+  ct.chunk_base = t + 2 * n1;
+  ct.qchunk_base = t + 3 * n1;
+  ct.tile_base = t + 4 * n1;
+  ct.n_clouds = n_clouds;
+  return ct;
+}
+
+// Issues the whole pipeline on stream s. ev: 4 events (or nullptr) bracketing
+// build | partition | search.
+uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats) {
+  const uint32_t passes = sh.Q ? (sh.key_bits + 7) / 8 : 0;
+  uint32_t n = (sh.single ? 1 : 0) + 7 + 3 * passes + 1;   // tables, build, sort, gather
+  if (partitioned(pr) || feats) n += 1;                      // widths
+  n += partitioned(pr) ? 2 : 1;                              // search (+ fallback)
+  return n;
+}
+
+rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr,
+                  const float* d_pts, const float* d_qs, int32_t* d_out, cudaStream_t s,
+                  cudaEvent_t* ev, float* feats_out = nullptr, float* cellsz_out = nullptr) {
+  Counters* ctr = (Counters*)ws.counters.p;
+  const bool knn = pr.mode == RTNN_MODE_KNN;
+  const rtnn_tuning& tu = c->tuning;
+  if (ev) RTNN_CU(cudaEventRecord(ev[0], s), "event");
+  RTNN_CU(cudaMemsetAsync(ctr, 0, sizeof(Counters), s), "memset counters");
+  if (sh.single)
+    RTNN_CU(launch_single_tables((uint32_t*)ws.tables.p, (uint32_t)sh.N, (uint32_t)sh.Q, s), "tables");
+  const CloudTables t = tables_of(ws, sh.n_clouds);
+  const bool ap = ((uintptr_t)d_pts % 16) == 0, aq = ((uintptr_t)d_qs % 16) == 0;
+  uint32_t* cells = (uint32_t*)ws.cells.p;
+  CloudGrid* grids = (CloudGrid*)ws.grids.p;
+
+  RTNN_CU(launch_bbox(d_pts, sh.N, ap, t, sh.n_chunks, (uint32_t*)ws.bbox.p, s), "bbox");
+  RTNN_CU(launch_grid_plan(t, (const uint32_t*)ws.bbox.p, pr.radius, tu.cell_ratio,
+                           sh.cell_budget, sh.morton_bits, sh.cell_capacity, grids, ctr, s),
+          "grid plan");
+  RTNN_CU(launch_zero_cells(cells, ctr, c->n_sms, s), "zero cells");
+  RTNN_CU(launch_count(d_pts, sh.N, ap, t, sh.n_chunks, grids, cells, (uint32_t*)ws.rank.p, ctr, s),
+          "count");
+  RTNN_CU(launch_scan_excl(cells, 0, &ctr->total_cells, 1, sh.cell_capacity + 1,
+                           (uint64_t*)ws.scan_state.p, &ctr->scan_tiles[0], ctr, s),
+          "scan cells");
+  RTNN_CU(launch_scatter(d_pts, sh.N, ap, t, sh.n_chunks, grids, cells, (uint32_t*)ws.rank.p,
+                         (float4*)ws.spts.p, ctr, s),
+          "scatter");
+  RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.morton_bits, sh.key64,
+                            ws.keys0.p, nullptr, s),
+          "query keys");
+  bool in1 = false;
+  RTNN_CU(radix_sort_pairs(sh.key64, ws.keys0.p, (uint32_t*)ws.vals0.p, ws.keys1.p,
+                           (uint32_t*)ws.vals1.p, (uint32_t)sh.Q, sh.key_bits, true,
+                           (uint32_t*)ws.hist.p, (uint64_t*)ws.scan_state.p, &ctr->scan_tiles[1],
+                           ctr, &in1, s),
+          "radix sort");
+  const uint32_t* order = (const uint32_t*)(in1 ? ws.vals1.p : ws.vals0.p);
+  RTNN_CU(launch_gather_queries(d_qs, order, (uint32_t)sh.Q, (float4*)ws.sq.p, c->n_sms, s),
+          "gather queries");
+  if (ev) RTNN_CU(cudaEventRecord(ev[1], s), "event");
+
+  const bool part = partitioned(pr);
+  if (part || feats_out) {
+    WidthArgs w{};
+    w.t = t;
+    w.grids = grids;
+    w.cells = cells;
+    w.sq = (const float4*)ws.sq.p;
+    w.total_cells = &ctr->total_cells;
+    w.n_queries = (uint32_t)sh.Q;
+    w.radius = pr.radius;
+    w.need = pr.k + 1;
+    w.alpha = 1.24f;   // equal-volume radius of a (2s+2)-cell cube, util.cpp:422-426
+    w.model = (pr.flags & RTNN_FLAG_LEARNED) ? (const float*)c->model.p : nullptr;
+    w.margin = tu.width_margin;
+    w.qwidth = part ? (float*)ws.qwidth.p : nullptr;
+    w.feats = feats_out;
+    w.cellsz = cellsz_out;
+    if (!part) {   // features only: widths land in a scratch buffer
+      RTNN_CU(ensure(ws.qwidth, std::max<uint64_t>(sh.Q, 1) * 4), "alloc widths");
+      w.qwidth = (float*)ws.qwidth.p;
+    }
+    RTNN_CU(launch_widths(w, c->n_sms, s), "widths");
+  }
+  if (ev) RTNN_CU(cudaEventRecord(ev[2], s), "event");
+
+  SearchArgs a{};
+  a.t = t;
+  a.grids = grids;
+  a.cells = cells;
+  a.spts = (const float4*)ws.spts.p;
+  a.sq = (const float4*)ws.sq.p;
+  a.qwidth = part ? (const float*)ws.qwidth.p : nullptr;
+  a.fb_pos = (const uint32_t*)ws.fbpos.p;
+  a.fb_cloud = (const uint32_t*)ws.fbcloud.p;
+  a.fb_out_pos = (uint32_t*)ws.fbpos.p;
+  a.fb_out_cloud = (uint32_t*)ws.fbcloud.p;
+  a.out = d_out;
+  a.ctr = ctr;
+  a.work = &ctr->work[0];
+  a.n_tiles = sh.n_tiles;
+  a.radius = pr.radius;
+  a.r2 = pr.radius * pr.radius;
+  a.k = pr.k;
+  a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
+            ((pr.flags & RTNN_FLAG_LOCAL_INDICES) ? kSearchLocalIndices : 0u);
+  a.fallback_pass = false;
+  const int wpb = (int)std::max(1u, std::min(8u, tu.warps_per_block));
+  int bps = search_blocks_per_sm(knn, pr.k, wpb);
+  if (tu.blocks_per_sm > 0) bps = std::min(bps, (int)tu.blocks_per_sm);
+  const uint64_t persistent = (uint64_t)c->n_sms * bps;
+  const uint64_t need_blocks = (sh.n_tiles + wpb - 1) / wpb;
+  const unsigned blocks1 = (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
+  RTNN_CU(launch_search(knn, a, blocks1, wpb, s), "search");
+  if (part) {
+    a.fallback_pass = true;
+    a.work = &ctr->work[1];
+    a.qwidth = nullptr;
+    RTNN_CU(launch_search(knn, a, (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks)),
+                          wpb, s),
+            "fallback search");
+  }
+  if (ev) RTNN_CU(cudaEventRecord(ev[3], s), "event");
+  return RTNN_OK;
+}
+
+rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& sh,
+                      const Params& pr, rtnn_stats* stats, bool timed) {
+  RTNN_CU(cudaMemcpyAsync(c->h_ctr, ws.counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s),
+          "read counters");
+  RTNN_CU(cudaMemcpyAsync(c->h_grid, ws.grids.p, sizeof(CloudGrid), cudaMemcpyDeviceToHost, s),
+          "read grid");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  const Counters& h = *c->h_ctr;
+  if (h.error == kErrScanTimeout)
+    return fail(c, RTNN_ERR_DEVICE_TIMEOUT, "scan look-back gave up waiting on tile " + std::to_string(h.error_info));
+  if (h.error == kErrCellCapacity)
+    return fail(c, RTNN_ERR_INTERNAL, "grid plan exceeded its cell capacity (cloud " + std::to_string(h.error_info) + ")");
+  if (h.error == kErrIndexRange)
+    return fail(c, RTNN_ERR_INTERNAL, "device index check failed (element " + std::to_string(h.error_info) + ")");
+  if (h.error != 0) return fail(c, RTNN_ERR_INTERNAL, "device error " + std::to_string(h.error));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->n_points = sh.N;
+    stats->n_queries = sh.Q;
+    stats->n_clouds = sh.n_clouds;
+    stats->n_buckets = partitioned(pr) ? 2 : 1;
+    stats->n_fallback = h.fb_count;
+    stats->n_tiles = sh.n_tiles;
+    stats->n_cells = h.total_cells;
+    stats->cell_size = c->h_grid->cell;
+    stats->grid_dims[0] = (uint32_t)c->h_grid->dx;
+    stats->grid_dims[1] = (uint32_t)c->h_grid->dy;
+    stats->grid_dims[2] = (uint32_t)c->h_grid->dz;
+    stats->n_launches = launches_of(sh, pr, false);
+    if (timed) {
+      cudaEventElapsedTime(&stats->ms_build, c->ev[0], c->ev[1]);
+      cudaEventElapsedTime(&stats->ms_partition, c->ev[1], c->ev[2]);
+      cudaEventElapsedTime(&stats->ms_search, c->ev[2], c->ev[3]);
+      cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[3]);
+    }
+  }
+  return RTNN_OK;
+}
+
+cudaStream_t stream_of(rtnn_ctx* c) { return c->stream ? c->stream : c->own; }
+
+// Full search with optional host staging. feats/cellsz (device) collect MLP features.
+rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const float* points,
+                       const float* queries, int32_t* out, rtnn_stats* stats,
+                       float* feats = nullptr, float* cellsz = nullptr) {
+  cudaStream_t s = stream_of(c);
+  const bool dev = (pr.flags & RTNN_FLAG_DEVICE_POINTERS) != 0;
+  const bool same = (queries == nullptr);
+  if (sh.Q == 0) return RTNN_OK;
+  rtnn_status st = reserve(c, c->ws, sh, pr);
+  if (st != RTNN_OK) return st;
+  const float* d_pts = points;
+  const float* d_qs = same ? points : queries;
+  int32_t* d_out = out;
+  const size_t out_bytes = (size_t)sh.Q * pr.k * sizeof(int32_t);
+  if (!dev) {
+    RTNN_CU(ensure(c->ws.in_pts, std::max<uint64_t>(sh.N, 1) * 12), "alloc points");
+    RTNN_CU(cudaMemcpyAsync(c->ws.in_pts.p, points, sh.N * 12, cudaMemcpyHostToDevice, s), "copy points");
+    d_pts = (const float*)c->ws.in_pts.p;
+    if (same) {
+      d_qs = d_pts;
+    } else {
+      RTNN_CU(ensure(c->ws.in_qs, sh.Q * 12), "alloc queries");
+      RTNN_CU(cudaMemcpyAsync(c->ws.in_qs.p, queries, sh.Q * 12, cudaMemcpyHostToDevice, s), "copy queries");
+      d_qs = (const float*)c->ws.in_qs.p;
+    }
+    RTNN_CU(ensure(c->ws.out, out_bytes), "alloc output");
+    d_out = (int32_t*)c->ws.out.p;
+  }
+  if (sh.N == 0) {
+    RTNN_CU(cudaMemsetAsync(d_out, 0xff, out_bytes, s), "fill output");
+  } else {
+    st = issue(c, c->ws, sh, pr, d_pts, d_qs, d_out, s, c->ev, feats, cellsz);
+    if (st != RTNN_OK) return st;
+  }
+  if (!dev) RTNN_CU(cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, s), "copy output");
+  if (sh.N == 0) {
+    RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+    if (stats) {
+      std::memset(stats, 0, sizeof(*stats));
+      stats->n_queries = sh.Q;
+      stats->n_clouds = sh.n_clouds;
+    }
+    return RTNN_OK;
+  }
+  return read_back(c, c->ws, s, sh, pr, stats, true);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rtnn_version(void) { return "rtnn_b200 0.1.0 (sm_100a)"; }
+
+int rtnn_k_supported(uint32_t k) { return (k >= 1 && k <= RTNN_MAX_K) ? 1 : 0; }
+
+rtnn_status rtnn_create(rtnn_ctx** out, int device) {
+  if (!out) return RTNN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return RTNN_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) return RTNN_ERR_NO_DEVICE;
+  rtnn_ctx* c = new rtnn_ctx();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->n_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_ctr, sizeof(Counters));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_grid, sizeof(CloudGrid));
+  if (e == cudaSuccess) e = search_prepare(device);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    rtnn_destroy(c);
+    return RTNN_ERR_CUDA;
+  }
+  *out = c;
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_destroy(rtnn_ctx* c) {
+  if (!c) return RTNN_OK;
+  cudaSetDevice(c->device);
+  if (c->own) cudaStreamSynchronize(c->own);
+  c->ws.release_all();
+  release(c->model);
+  release(c->train_grad);
+  release(c->train_m);
+  release(c->train_v);
+  release(c->train_loss);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  if (c->h_grid) cudaFreeHost(c->h_grid);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return RTNN_OK;
+}
+
+const char* rtnn_last_error(const rtnn_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+rtnn_status rtnn_set_stream(rtnn_ctx* c, void* stream) {
+  if (!c) return RTNN_ERR_INVALID_ARGUMENT;
+  c->stream = (cudaStream_t)stream;
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_get_tuning(const rtnn_ctx* c, rtnn_tuning* t) {
+  if (!c || !t) return RTNN_ERR_INVALID_ARGUMENT;
+  *t = c->tuning;
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
+  if (!c || !t) return RTNN_ERR_INVALID_ARGUMENT;
+  if (!(t->cell_ratio > 0.f && t->cell_ratio <= 64.f) || !(t->cell_budget > 0.f) ||
+      t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f))
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
+  c->tuning = *t;
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_search(rtnn_ctx* c, const float* points, uint64_t n_points, const float* queries,
+                        uint64_t n_queries, rtnn_mode mode, float radius, uint32_t k,
+                        uint32_t flags, int32_t* out, rtnn_stats* stats) {
+  if (!c) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  if (mode != RTNN_MODE_RADIUS && mode != RTNN_MODE_KNN)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "mode must be RTNN_MODE_RADIUS or RTNN_MODE_KNN");
+  if (queries == nullptr) n_queries = n_points;
+  rtnn_status st = check_args(c, n_points, n_queries, radius, k, flags);
+  if (st != RTNN_OK) return st;
+  if (n_points > 0 && !points) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "points is NULL");
+  if (n_queries > 0 && !out) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "out is NULL");
+  if (flags & RTNN_FLAG_LOCAL_INDICES) flags &= ~RTNN_FLAG_LOCAL_INDICES;  // one cloud: same
+  cudaSetDevice(c->device);
+  const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
+  const Params pr{mode, radius, k, flags};
+  return run_search(c, sh, pr, points, queries, out, stats);
+}
+
+rtnn_status rtnn_search_batched(rtnn_ctx* c, const float* points, const uint64_t* point_offsets,
+                                uint32_t n_clouds, const float* queries,
+                                const uint64_t* query_offsets, rtnn_mode mode, float radius,
+                                uint32_t k, uint32_t flags, int32_t* out, rtnn_stats* stats) {
+  if (!c) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  if (mode != RTNN_MODE_RADIUS && mode != RTNN_MODE_KNN)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "mode must be RTNN_MODE_RADIUS or RTNN_MODE_KNN");
+  Shapes sh;
+  rtnn_status st = batched_shapes(c, point_offsets, n_clouds, queries ? query_offsets : nullptr,
+                                  c->tuning, sh);
+  if (st != RTNN_OK) return st;
+  if (queries && !query_offsets) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "query_offsets is NULL");
+  st = check_args(c, sh.N, sh.Q, radius, k, flags);
+  if (st != RTNN_OK) return st;
+  if (sh.N > 0 && !points) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "points is NULL");
+  if (sh.Q > 0 && !out) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "out is NULL");
+  cudaSetDevice(c->device);
+  const Params pr{mode, radius, k, flags};
+  st = reserve(c, c->ws, sh, pr);
+  if (st != RTNN_OK) return st;
+  cudaStream_t s = stream_of(c);
+  RTNN_CU(cudaMemcpyAsync(c->ws.tables.p, sh.tab.data(), sh.tab.size() * 4, cudaMemcpyHostToDevice, s),
+          "copy tables");
+  return run_search(c, sh, pr, points, queries, out, stats);
+}
+
+// ---- plans (CUDA graph) ------------------------------------------------------------
+
+rtnn_status rtnn_plan_create(rtnn_ctx* c, rtnn_plan** plan, const uint64_t* point_offsets,
+                             uint32_t n_clouds, const uint64_t* query_offsets, rtnn_mode mode,
+                             float radius, uint32_t k, uint32_t flags, int use_graph) {
+  if (!c || !plan) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  *plan = nullptr;
+  if (mode != RTNN_MODE_RADIUS && mode != RTNN_MODE_KNN)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "mode must be RTNN_MODE_RADIUS or RTNN_MODE_KNN");
+  rtnn_plan* p = new rtnn_plan();
+  p->ctx = c;
+  rtnn_status st = batched_shapes(c, point_offsets, n_clouds, query_offsets, c->tuning, p->sh);
+  if (st == RTNN_OK) st = check_args(c, p->sh.N, p->sh.Q, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS);
+  if (st == RTNN_OK && (p->sh.N == 0 || p->sh.Q == 0))
+    st = fail(c, RTNN_ERR_INVALID_ARGUMENT, "a plan needs at least one point and one query");
+  if (st != RTNN_OK) { delete p; return st; }
+  p->pr = Params{mode, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS};
+  p->use_graph = use_graph != 0;
+  cudaSetDevice(c->device);
+  st = reserve(c, p->ws, p->sh, p->pr);
+  if (st == RTNN_OK) {
+    cudaError_t e = cudaMemcpy(p->ws.tables.p, p->sh.tab.data(), p->sh.tab.size() * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) st = cuda_fail(c, e, "copy tables");
+  }
+  if (st != RTNN_OK) {
+    p->ws.release_all();
+    delete p;
+    return st;
+  }
+  *plan = p;
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_plan_execute(rtnn_plan* p, const float* d_points, const float* d_queries,
+                              int32_t* d_out, rtnn_stats* stats) {
+  if (!p) return RTNN_ERR_INVALID_ARGUMENT;
+  rtnn_ctx* c = p->ctx;
+  c->err.clear();
+  if (!d_points || !d_out) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "NULL device pointer");
+  if ((p->pr.flags & RTNN_FLAG_LEARNED) && !c->has_model)
+    return fail(c, RTNN_ERR_NO_MODEL, "RTNN_FLAG_LEARNED needs a width model");
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  const float* d_qs = d_queries ? d_queries : d_points;
+  if (!p->use_graph) {
+    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, c->ev);
+    if (st != RTNN_OK) return st;
+    return read_back(c, p->ws, s, p->sh, p->pr, stats, true);
+  }
+  if (!p->exec || p->g_pts != d_points || p->g_qs != d_qs || p->g_out != d_out) {
+    if (p->exec) { cudaGraphExecDestroy(p->exec); p->exec = nullptr; }
+    if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+    RTNN_CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (st != RTNN_OK) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return cuda_fail(c, e, "end capture");
+    p->graph = g;
+    RTNN_CU(cudaGraphInstantiate(&p->exec, g, 0), "instantiate graph");
+    p->g_pts = d_points;
+    p->g_qs = d_qs;
+    p->g_out = d_out;
+  }
+  RTNN_CU(cudaEventRecord(c->ev[0], s), "event");
+  RTNN_CU(cudaGraphLaunch(p->exec, s), "graph launch");
+  RTNN_CU(cudaEventRecord(c->ev[3], s), "event");
+  rtnn_status st = read_back(c, p->ws, s, p->sh, p->pr, stats, false);
+  if (st == RTNN_OK && stats) cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[3]);
+  return st;
+}
+
+rtnn_status rtnn_plan_destroy(rtnn_plan* p) {
+  if (!p) return RTNN_OK;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(stream_of(p->ctx));
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->ws.release_all();
+  delete p;
+  return RTNN_OK;
+}
+
+// ---- learned widths -------------------------------------------------------------------
+
+uint32_t rtnn_model_size(void) { return (uint32_t)kModelParams; }
+
+rtnn_status rtnn_model_set(rtnn_ctx* c, const float* params, uint32_t n) {
+  if (!c || !params) return RTNN_ERR_INVALID_ARGUMENT;
+  if (n != (uint32_t)kModelParams)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "model must have rtnn_model_size() floats");
+  cudaSetDevice(c->device);
+  RTNN_CU(ensure(c->model, kModelParams * 4), "alloc model");
+  RTNN_CU(cudaMemcpy(c->model.p, params, kModelParams * 4, cudaMemcpyHostToDevice), "copy model");
+  c->has_model = true;
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_model_get(rtnn_ctx* c, float* params, uint32_t n) {
+  if (!c || !params) return RTNN_ERR_INVALID_ARGUMENT;
+  if (!c->has_model) return fail(c, RTNN_ERR_NO_MODEL, "no model loaded");
+  if (n != (uint32_t)kModelParams)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "model must have rtnn_model_size() floats");
+  cudaSetDevice(c->device);
+  RTNN_CU(cudaMemcpy(params, c->model.p, kModelParams * 4, cudaMemcpyDeviceToHost), "copy model");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_collect_training(rtnn_ctx* c, const float* d_points, uint64_t n_points,
+                                  const float* d_queries, uint64_t n_queries, rtnn_mode mode,
+                                  float radius, uint32_t k, float* d_feats, float* d_target) {
+  if (!c || !d_points || !d_feats || !d_target) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  if (d_queries == nullptr) n_queries = n_points;
+  const uint32_t flags = RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_SORTED_ROWS;
+  rtnn_status st = check_args(c, n_points, n_queries, radius, k, flags);
+  if (st != RTNN_OK) return st;
+  if (n_points == 0 || n_queries == 0) return RTNN_OK;
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  RTNN_CU(ensure(c->ws.out, (size_t)n_queries * k * 4), "alloc rows");
+  RTNN_CU(ensure(c->ws.cellsz, n_queries * 4), "alloc cell sizes");
+  RTNN_CU(ensure(c->ws.kth, n_queries * 4), "alloc kth");
+  const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
+  const Params pr{mode, radius, k, flags};
+  int32_t* rows = (int32_t*)c->ws.out.p;
+  st = run_search(c, sh, pr, d_points, d_queries, rows, nullptr, d_feats, (float*)c->ws.cellsz.p);
+  if (st != RTNN_OK) return st;
+  const float* qs = d_queries ? d_queries : d_points;
+  RTNN_CU(launch_kth_dist(rows, (uint32_t)n_queries, k, d_points, qs, (float*)c->ws.kth.p, s), "kth");
+  // target = log(kth / cell); queries with < K neighbors inside r get log(1.5 r / cell)
+  std::vector<float> kth(n_queries), cz(n_queries);
+  RTNN_CU(cudaMemcpyAsync(kth.data(), c->ws.kth.p, n_queries * 4, cudaMemcpyDeviceToHost, s), "copy");
+  RTNN_CU(cudaMemcpyAsync(cz.data(), c->ws.cellsz.p, n_queries * 4, cudaMemcpyDeviceToHost, s), "copy");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  std::vector<float> tgt(n_queries);
+  for (uint64_t i = 0; i < n_queries; ++i) {
+    const float d = kth[i] >= 0.f ? std::max(kth[i], 1e-6f * radius) : 1.5f * radius;
+    tgt[i] = std::log(d / cz[i]);
+  }
+  RTNN_CU(cudaMemcpyAsync(d_target, tgt.data(), n_queries * 4, cudaMemcpyHostToDevice, s), "copy");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_mlp_loss_grad(rtnn_ctx* c, const float* d_params, const float* d_feats,
+                               const float* d_target, uint32_t n, float* d_grad, float* d_loss) {
+  if (!c || !d_params || !d_feats || !d_target || !d_grad || !d_loss) return RTNN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  RTNN_CU(cudaMemsetAsync(d_grad, 0, kTrainParams * 4, s), "memset");
+  RTNN_CU(cudaMemsetAsync(d_loss, 0, 4, s), "memset");
+  MlpBatch b{d_feats, d_target, n};
+  RTNN_CU(launch_mlp_loss_grad(d_params, b, d_grad, d_loss, c->n_sms, s), "loss/grad");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_mlp_forward(rtnn_ctx* c, const float* d_params, const float* d_feats, uint32_t n,
+                             float* d_y) {
+  if (!c || !d_params || !d_feats || !d_y) return RTNN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  RTNN_CU(launch_mlp_forward(d_params, d_feats, n, d_y, c->n_sms, s), "forward");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_mlp_adam_step(rtnn_ctx* c, float* d_params, const float* d_grad, float* d_m,
+                               float* d_v, float lr, uint32_t step, float grad_scale) {
+  if (!c || !d_params || !d_grad || !d_m || !d_v || step == 0) return RTNN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  RTNN_CU(launch_mlp_adam(d_params, d_grad, d_m, d_v, lr, 0.9f, 0.999f, 1e-8f, step, grad_scale, s),
+          "adam");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_model_train(rtnn_ctx* c, const float* d_feats, const float* d_target,
+                             uint64_t n, uint32_t epochs, uint32_t batch, float lr,
+                             uint64_t seed, float* loss_per_epoch) {
+  if (!c || !d_feats || !d_target || n == 0 || epochs == 0 || batch == 0)
+    return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  // input / output normalisation from the data (host), He-initialised weights
+  std::vector<float> f(n * kFeatDim), t(n);
+  RTNN_CU(cudaMemcpyAsync(f.data(), d_feats, f.size() * 4, cudaMemcpyDeviceToHost, s), "copy");
+  RTNN_CU(cudaMemcpyAsync(t.data(), d_target, t.size() * 4, cudaMemcpyDeviceToHost, s), "copy");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  std::vector<float> P(kModelParams, 0.f);
+  for (int j = 0; j < kFeatDim; ++j) {
+    double m = 0, v = 0;
+    for (uint64_t i = 0; i < n; ++i) m += f[i * kFeatDim + j];
+    m /= (double)n;
+    for (uint64_t i = 0; i < n; ++i) { const double d = f[i * kFeatDim + j] - m; v += d * d; }
+    v /= (double)n;
+    P[j] = (float)m;
+    P[kFeatDim + j] = (float)std::max(std::sqrt(v), 1e-3);
+  }
+  {
+    double m = 0, v = 0;
+    for (uint64_t i = 0; i < n; ++i) m += t[i];
+    m /= (double)n;
+    for (uint64_t i = 0; i < n; ++i) { const double d = t[i] - m; v += d * d; }
+    P[2 * kFeatDim] = (float)m;
+    P[2 * kFeatDim + 1] = (float)std::max(std::sqrt(v / (double)n), 1e-3);
+  }
+  uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+  auto unif = [&]() {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    return ((st >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;
+  };
+  float* T = P.data() + kNormParams;
+  const float s1 = std::sqrt(6.0f / kFeatDim), s2 = std::sqrt(6.0f / kHidden);
+  for (int i = 0; i < kHidden * kFeatDim; ++i) T[i] = (float)(unif() * s1);
+  float* W2 = T + kHidden * kFeatDim + kHidden;
+  for (int i = 0; i < kHidden * kHidden; ++i) W2[i] = (float)(unif() * s2);
+  float* W3 = W2 + kHidden * kHidden + kHidden;
+  for (int i = 0; i < kHidden; ++i) W3[i] = (float)(unif() * s2 * 0.5f);
+  RTNN_CU(ensure(c->model, kModelParams * 4), "alloc model");
+  RTNN_CU(ensure(c->train_grad, kTrainParams * 4), "alloc grad");
+  RTNN_CU(ensure(c->train_m, kTrainParams * 4), "alloc adam");
+  RTNN_CU(ensure(c->train_v, kTrainParams * 4), "alloc adam");
+  RTNN_CU(ensure(c->train_loss, 4 * epochs + 16), "alloc loss");
+  float* dP = (float*)c->model.p;
+  RTNN_CU(cudaMemcpyAsync(dP, P.data(), kModelParams * 4, cudaMemcpyHostToDevice, s), "copy");
+  RTNN_CU(cudaMemsetAsync(c->train_m.p, 0, kTrainParams * 4, s), "memset");
+  RTNN_CU(cudaMemsetAsync(c->train_v.p, 0, kTrainParams * 4, s), "memset");
+  RTNN_CU(cudaMemsetAsync(c->train_loss.p, 0, 4 * epochs, s), "memset");
+  float* dloss = (float*)c->train_loss.p;
+  uint32_t step = 0;
+  for (uint32_t ep = 0; ep < epochs; ++ep) {
+    for (uint64_t b0 = 0; b0 < n; b0 += batch) {
+      const uint32_t nb = (uint32_t)std::min<uint64_t>(batch, n - b0);
+      RTNN_CU(cudaMemsetAsync(c->train_grad.p, 0, kTrainParams * 4, s), "memset");
+      MlpBatch b{d_feats + b0 * kFeatDim, d_target + b0, nb};
+      RTNN_CU(launch_mlp_loss_grad(dP, b, (float*)c->train_grad.p, dloss + ep, c->n_sms, s), "loss/grad");
+      RTNN_CU(launch_mlp_adam(dP, (const float*)c->train_grad.p, (float*)c->train_m.p,
+                              (float*)c->train_v.p, lr, 0.9f, 0.999f, 1e-8f, ++step, 1.0f / nb, s),
+              "adam");
+    }
+  }
+  if (loss_per_epoch) {
+    RTNN_CU(cudaMemcpyAsync(loss_per_epoch, dloss, 4 * epochs, cudaMemcpyDeviceToHost, s), "copy");
+  }
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  if (loss_per_epoch)
+    for (uint32_t ep = 0; ep < epochs; ++ep) loss_per_epoch[ep] /= (float)n;
+  c->has_model = true;
+  return RTNN_OK;
+}
+
+}  // extern "C"

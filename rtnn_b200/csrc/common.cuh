@@ -1,0 +1,134 @@
+// common.cuh -- shared device structs and helpers of the B200 neighbor-search engine.
+//
+// Layout in HBM (one pipeline = one set of clouds; a single cloud is a batch of one):
+//   points (caller)    AoS float3, 12 B/point, read with 16-byte vector loads.
+//   spts               float4 {x, y, z, original index bits}, 16 B/point, sorted by
+//                      grid cell (raster order inside each cloud, clouds in order).
+//   cells              uint32 per cell + 1: per-cell counts, scanned in place into
+//                      cell start offsets (cells[total] == number of points).
+//   sq                 float4 {x, y, z, original query index bits} in Morton order.
+//   out (caller)       int32 [Q][K], -1 in unused slots.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rtnn {
+
+constexpr int kChunk = 2048;        // points per block of the per-point kernels
+constexpr int kTile = 32;           // queries per search work item (one warp)
+constexpr int kScanItems = 16;      // items per thread of the scan
+constexpr int kScanThreads = 256;
+constexpr int kScanTile = kScanItems * kScanThreads;   // 4096
+constexpr int kRadixThreads = 256;  // 8 warps
+constexpr int kRadixItems = 16;     // per lane, per warp sub-tile of 512
+constexpr int kRadixTile = kRadixThreads * kRadixItems; // 4096 keys per block
+constexpr int kMaxK = 128;
+
+// Device error codes (first one wins, written with atomicCAS into Counters::error).
+enum DevError : uint32_t {
+  kErrNone = 0,
+  kErrScanTimeout = 1,     // decoupled look-back predecessor never published
+  kErrCellCapacity = 2,    // grid plan needed more cells than were allocated
+  kErrIndexRange = 3,      // a computed index fell outside its buffer (access skipped)
+};
+
+// Per-cloud uniform grid (written on the device by k_grid_plan).
+struct __align__(16) CloudGrid {
+  float ox, oy, oz;      // grid origin = min corner of the cloud's points
+  float cell;            // cell edge
+  float inv_cell;        // 1 / cell
+  int dx, dy, dz;        // cells per axis
+  uint32_t cell_base;    // first cell of this cloud in the global cell array
+  uint32_t morton_shift; // cell coords >> shift before Morton interleaving
+  uint32_t n_cells;      // dx * dy * dz
+  uint32_t pad;
+};
+
+// Small counters zeroed at the start of every pipeline run.
+struct Counters {
+  uint32_t error;          // DevError
+  uint32_t error_info;     // extra detail (e.g. scan tile that timed out)
+  uint32_t work[4];        // persistent-kernel work queues
+  uint32_t fb_count;       // queries appended to the fallback list
+  uint32_t total_cells;    // sum of cloud cells (written by k_grid_plan)
+  uint32_t scan_tiles[16]; // dynamic tile counters, one per scan invocation
+  uint64_t n_hits;         // optional statistics
+  uint32_t pad[6];
+};
+
+// Tables describing the clouds of one pipeline (all device arrays of n_clouds + 1).
+struct CloudTables {
+  const uint32_t* point_off;   // first point of cloud c; [n] = N
+  const uint32_t* query_off;   // first query of cloud c; [n] = Q
+  const uint32_t* chunk_base;  // first point chunk of cloud c; [n] = point chunks
+  const uint32_t* qchunk_base; // first query chunk of cloud c; [n] = query chunks
+  const uint32_t* tile_base;   // first 32-query tile of cloud c; [n] = tiles
+  uint32_t n_clouds;
+};
+
+__device__ __forceinline__ void set_error(Counters* c, uint32_t code, uint32_t info) {
+  if (atomicCAS(&c->error, 0u, code) == 0u) c->error_info = info;
+}
+
+// Largest c with base[c] <= x (base ascending, base[0] == 0, n_clouds + 1 entries).
+__device__ __forceinline__ uint32_t find_cloud(const uint32_t* base, uint32_t n_clouds,
+                                               uint32_t x) {
+  uint32_t lo = 0, hi = n_clouds;  // invariant: base[lo] <= x < base[hi] (base[n] is total)
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(base + mid) <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Order-preserving map float -> uint32 (for atomicMin/Max on floats).
+__device__ __forceinline__ uint32_t f2o(float f) {
+  uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float o2f(uint32_t o) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+#else
+  uint32_t b = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+  float f; __builtin_memcpy(&f, &b, 4); return f;
+#endif
+}
+
+// Squared distance with the reference's operation order and rounding:
+// dot(d, d) = d.x*d.x + d.y*d.y + d.z*d.z evaluated left to right, every product and
+// sum rounded to FP32, no FMA (src/sutil/vec_math.h:527-530, check.cpp:36-37).
+__device__ __forceinline__ float dist2_ref(float qx, float qy, float qz,
+                                          float px, float py, float pz) {
+  float dx = __fsub_rn(qx, px), dy = __fsub_rn(qy, py), dz = __fsub_rn(qz, pz);
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// Cell coordinate of v along one axis: floor((v - o) * inv), clamped to [0, d-1].
+// The same monotone expression bins points and bounds query ranges.
+__device__ __forceinline__ float cell_coord_f(float v, float o, float inv) {
+  return floorf(__fmul_rn(__fsub_rn(v, o), inv));
+}
+__device__ __forceinline__ int clamp_cell(float c, int d) {
+  c = fminf(fmaxf(c, 0.f), (float)(d - 1));  // NaN -> 0 via fmaxf
+  return (int)c;
+}
+
+// 10-bit-per-axis Morton interleave (bit i of x -> bit 3i).
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+__device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m;
+}
+
+}  // namespace rtnn

@@ -1,0 +1,124 @@
+// kernels.h -- host-side launchers of the device kernels (one translation unit each).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace rtnn {
+
+constexpr uint32_t kSearchSortedRows = 1u;
+constexpr uint32_t kSearchLocalIndices = 2u;
+
+struct SearchArgs {
+  CloudTables t;
+  const CloudGrid* grids;
+  const uint32_t* cells;       // cell start offsets (scanned counts)
+  const float4* spts;          // cell-sorted points {x, y, z, index}
+  const float4* sq;            // Morton-sorted queries {x, y, z, query index}
+  const float* qwidth;         // per sorted query search width; nullptr: full radius
+  const uint32_t* fb_pos;      // fallback pass: sorted positions to re-search
+  const uint32_t* fb_cloud;    //                and their clouds
+  uint32_t* fb_out_pos;        // first pass: where narrowed-but-short queries go
+  uint32_t* fb_out_cloud;
+  int32_t* out;                // [Q][k]
+  Counters* ctr;
+  uint32_t* work;              // work-queue counter of this pass
+  uint32_t n_tiles;            // first pass tile count
+  float radius;                // user radius r
+  float r2;                    // fl(r * r)
+  uint32_t k;
+  uint32_t flags;              // kSearch*
+  bool fallback_pass;
+};
+
+// scan.cu
+uint64_t scan_tiles_for(uint64_t n);
+cudaError_t launch_scan_excl(uint32_t* data, uint64_t n_host, const uint32_t* n_dev,
+                             uint32_t n_add, uint64_t max_n, uint64_t* tile_state,
+                             uint32_t* tile_counter, Counters* ctr, cudaStream_t s);
+
+// radix_sort.cu
+uint32_t radix_tiles_for(uint64_t n);
+cudaError_t radix_sort_pairs(bool key64, void* keys0, uint32_t* vals0, void* keys1,
+                             uint32_t* vals1, uint32_t n, uint32_t bits, bool identity_values,
+                             uint32_t* hist, uint64_t* scan_state, uint32_t* scan_counters,
+                             Counters* ctr, bool* result_in_1, cudaStream_t s);
+
+// build_grid.cu
+cudaError_t launch_single_tables(uint32_t* tab, uint32_t n_points, uint32_t n_queries,
+                                 cudaStream_t s);
+cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
+                        uint32_t n_chunks, uint32_t* bbox, cudaStream_t s);
+cudaError_t launch_grid_plan(const CloudTables& t, const uint32_t* bbox, float radius,
+                             float cell_ratio, float cell_budget, uint32_t morton_bits,
+                             uint64_t cell_capacity, CloudGrid* grids, Counters* ctr,
+                             cudaStream_t s);
+cudaError_t launch_zero_cells(uint32_t* cells, const Counters* ctr, int n_sms, cudaStream_t s);
+cudaError_t launch_count(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
+                         uint32_t n_chunks, const CloudGrid* grids, uint32_t* cells,
+                         uint32_t* rank, Counters* ctr, cudaStream_t s);
+cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
+                           const CloudTables& t, uint32_t n_chunks, const CloudGrid* grids,
+                           const uint32_t* cells, const uint32_t* rank, float4* spts,
+                           Counters* ctr, cudaStream_t s);
+cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
+                              const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
+                              uint32_t morton_bits, bool key64, void* keys, uint32_t* vals,
+                              cudaStream_t s);
+cudaError_t launch_gather_queries(const float* xyz, const uint32_t* order, uint32_t n,
+                                  float4* sq, int n_sms, cudaStream_t s);
+
+// search.cu
+size_t search_smem_bytes(uint32_t k, int warps_per_block);
+cudaError_t search_prepare(int device);
+int search_blocks_per_sm(bool knn, uint32_t k, int warps_per_block);
+cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
+                          cudaStream_t s);
+
+// partition.cu -- density buckets: per-query search widths (analytic or learned MLP)
+constexpr int kShells = 3;                 // box counts N_0..N_2 around a query's cell
+constexpr int kFeatDim = 6;                // MLP input features per query
+constexpr int kHidden = 32;                // MLP hidden width (two hidden layers)
+// parameter layout (floats): in_mean[F] in_std[F] out_mean out_std | W1[H][F] b1[H]
+// W2[H][H] b2[H] W3[H] b3  -- only the part after '|' is trained
+constexpr int kNormParams = 2 * kFeatDim + 2;
+constexpr int kTrainParams = kHidden * kFeatDim + kHidden + kHidden * kHidden + kHidden + kHidden + 1;
+constexpr int kModelParams = kNormParams + kTrainParams;
+
+struct WidthArgs {
+  CloudTables t;
+  const CloudGrid* grids;
+  const uint32_t* cells;
+  const float4* sq;
+  const uint32_t* total_cells;  // cells in use (device)
+  uint32_t n_queries;
+  float radius;
+  uint32_t need;          // points a width must enclose (K + 1)
+  float alpha;            // analytic width = alpha * (s* + 1) * cell
+  const float* model;     // learned: MLP parameters (nullptr: analytic)
+  float margin;           // learned width = margin * predicted K-th distance
+  float* qwidth;          // out: per sorted query width (>= radius means full radius)
+  float* feats;           // optional out: [query index][kFeatDim] features (original order)
+  float* cellsz;          // optional out: [query index] cell edge of the query's cloud
+};
+cudaError_t launch_widths(const WidthArgs& a, int n_sms, cudaStream_t s);
+
+// MLP training (hand-written forward / backward / Adam), mlp.cu
+struct MlpBatch {
+  const float* feats;     // [n][kFeatDim]
+  const float* target;    // [n] log(K-th distance / cell)
+  uint32_t n;
+};
+cudaError_t launch_mlp_loss_grad(const float* params, const MlpBatch& b, float* grad,
+                                 float* loss_sum, int n_sms, cudaStream_t s);
+cudaError_t launch_mlp_adam(float* params, const float* grad, float* m, float* v, float lr,
+                            float beta1, float beta2, float eps, uint32_t step, float scale,
+                            cudaStream_t s);
+cudaError_t launch_mlp_forward(const float* params, const float* feats, uint32_t n, float* y,
+                               int n_sms, cudaStream_t s);
+cudaError_t launch_kth_dist(const int32_t* rows, uint32_t n_queries, uint32_t k,
+                            const float* points, const float* queries, float* kth_d,
+                            cudaStream_t s);
+
+}  // namespace rtnn

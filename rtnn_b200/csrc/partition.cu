@@ -1,0 +1,319 @@
+// partition.cu -- density buckets: a search width per query, analytic or learned.
+//
+// Replaces the reference's query partitioning (src/optixNSearch/):
+//   calcSearchSize / kGenCellMask (grid.cu:84-211, 354-382): per occupied cell, grow a
+//     box of cells shell by shell until it holds K+1 points; iter -> width
+//     (2*iter+2)*cellSize (getWidthFromIter, grid.cu:33-44);
+//   sortGenBatch / genBatches / radiusFromMegacell (sort.cpp:262-269, 346-391, 393-498):
+//     queries grouped by that width, each group launched with radius 0.62 * width
+//     (approxMode 2, radiusEquiVolume, util.cpp:422-426).
+// Here every query reads the box counts N_s (s = 0..2 cells around its cell) straight
+// from the scanned cell offsets (one subtraction per row of cells), and gets
+//   analytic: w = alpha * (s* + 1) * cell, s* = first s with N_s >= K + 1
+//             (alpha = 1.24 reproduces the reference's equal-volume radius), or
+//   learned:  w = margin * cell * exp(MLP(features)), the MLP predicting
+//             log(K-th neighbor distance / cell) from the bucket's occupancy histogram
+//             (shell counts) and its extent (cell / r).
+// A width >= r means "search at r". Exactness never depends on w: the search kernel
+// re-searches at r every query that finds fewer than K neighbors inside w.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rtnn {
+namespace {
+
+// ---- MLP (6 -> 32 -> 32 -> 1, ReLU) ------------------------------------------------
+struct MlpView {
+  const float* in_mean; const float* in_std; float out_mean, out_std;
+  const float* W1; const float* b1; const float* W2; const float* b2; const float* W3; float b3;
+};
+__device__ __forceinline__ MlpView mlp_view(const float* P) {
+  MlpView v;
+  v.in_mean = P; v.in_std = P + kFeatDim;
+  v.out_mean = P[2 * kFeatDim]; v.out_std = P[2 * kFeatDim + 1];
+  const float* T = P + kNormParams;
+  v.W1 = T; v.b1 = v.W1 + kHidden * kFeatDim;
+  v.W2 = v.b1 + kHidden; v.b2 = v.W2 + kHidden * kHidden;
+  v.W3 = v.b2 + kHidden; v.b3 = v.W3[kHidden];
+  return v;
+}
+
+// normalised output o (before out_mean/out_std) of one sample
+__device__ __forceinline__ float mlp_forward_norm(const MlpView& m, const float* x) {
+  float xn[kFeatDim];
+#pragma unroll
+  for (int f = 0; f < kFeatDim; ++f) xn[f] = (x[f] - m.in_mean[f]) / m.in_std[f];
+  float h1[kHidden];
+#pragma unroll
+  for (int j = 0; j < kHidden; ++j) {
+    float s = m.b1[j];
+#pragma unroll
+    for (int f = 0; f < kFeatDim; ++f) s = fmaf(m.W1[j * kFeatDim + f], xn[f], s);
+    h1[j] = fmaxf(s, 0.f);
+  }
+  float o = m.b3;
+#pragma unroll 1
+  for (int j = 0; j < kHidden; ++j) {
+    float s = m.b2[j];
+#pragma unroll
+    for (int i = 0; i < kHidden; ++i) s = fmaf(m.W2[j * kHidden + i], h1[i], s);
+    o = fmaf(m.W3[j], fmaxf(s, 0.f), o);
+  }
+  return o;
+}
+
+// Box count of cells [cx-s, cx+s] x [cy-s, cy+s] x [cz-s, cz+s] clipped to the grid.
+__device__ __forceinline__ uint32_t box_count(const CloudGrid& g, const uint32_t* cells,
+                                              int cx, int cy, int cz, int s) {
+  const int x0 = max(cx - s, 0), x1 = min(cx + s, g.dx - 1);
+  const int y0 = max(cy - s, 0), y1 = min(cy + s, g.dy - 1);
+  const int z0 = max(cz - s, 0), z1 = min(cz + s, g.dz - 1);
+  uint32_t n = 0;
+  for (int z = z0; z <= z1; ++z)
+    for (int y = y0; y <= y1; ++y) {
+      const uint32_t row = g.cell_base + ((uint32_t)z * (uint32_t)g.dy + (uint32_t)y) * (uint32_t)g.dx;
+      n += __ldg(cells + row + x1 + 1) - __ldg(cells + row + x0);
+    }
+  return n;
+}
+
+__global__ void __launch_bounds__(256)
+k_widths(WidthArgs a) {
+  __shared__ float s_model[kModelParams];
+  if (a.model) {
+    for (int i = threadIdx.x; i < kModelParams; i += blockDim.x) s_model[i] = a.model[i];
+    __syncthreads();
+  }
+  const MlpView mv = mlp_view(s_model);
+  const uint32_t total_cells = a.total_cells ? *a.total_cells : 0u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_queries;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t cloud = find_cloud(a.t.query_off, a.t.n_clouds, i);
+    const CloudGrid g = a.grids[cloud];
+    const float4 q = a.sq[i];
+    if ((uint64_t)g.cell_base + g.n_cells > (uint64_t)total_cells) {  // overran: full radius
+      a.qwidth[i] = a.radius;
+      continue;
+    }
+    const int cx = clamp_cell(cell_coord_f(q.x, g.ox, g.inv_cell), g.dx);
+    const int cy = clamp_cell(cell_coord_f(q.y, g.oy, g.inv_cell), g.dy);
+    const int cz = clamp_cell(cell_coord_f(q.z, g.oz, g.inv_cell), g.dz);
+    uint32_t N[kShells];
+#pragma unroll
+    for (int s = 0; s < kShells; ++s) N[s] = box_count(g, a.cells, cx, cy, cz, s);
+    float feat[kFeatDim];
+    feat[0] = log1pf((float)N[0]);
+    feat[1] = log1pf((float)(N[1] - N[0]));
+    feat[2] = log1pf((float)(N[2] - N[1]));
+    feat[3] = log1pf((float)N[2]);
+    feat[4] = logf(g.cell / a.radius);
+    feat[5] = logf((float)a.need);
+    float w;
+    if (a.model) {
+      const float o = mlp_forward_norm(mv, feat);
+      const float y = fmaf(o, mv.out_std, mv.out_mean);
+      w = a.margin * g.cell * expf(fminf(y, 30.f));
+    } else {
+      w = INFINITY;
+#pragma unroll
+      for (int s = 0; s < kShells; ++s)
+        if (w == INFINITY && N[s] >= a.need) w = a.alpha * (float)(s + 1) * g.cell;
+    }
+    a.qwidth[i] = (w < a.radius) ? w : a.radius;
+    const uint32_t qi = __float_as_uint(q.w);
+    if (a.feats) {
+#pragma unroll
+      for (int f = 0; f < kFeatDim; ++f) a.feats[(size_t)qi * kFeatDim + f] = feat[f];
+    }
+    if (a.cellsz) a.cellsz[qi] = g.cell;
+  }
+}
+
+// ---- training: loss and gradient of 0.5 * mean((o - t_n)^2) over a batch ---------
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(256)
+k_mlp_loss_grad(const float* __restrict__ P, MlpBatch b, float* __restrict__ grad,
+                float* __restrict__ loss_sum) {
+  __shared__ float s_p[kModelParams];
+  __shared__ float s_g[kTrainParams];
+  for (int i = threadIdx.x; i < kModelParams; i += blockDim.x) s_p[i] = P[i];
+  for (int i = threadIdx.x; i < kTrainParams; i += blockDim.x) s_g[i] = 0.f;
+  __syncthreads();
+  const MlpView m = mlp_view(s_p);
+  const int lane = threadIdx.x & 31;
+  float* gW1 = s_g;
+  float* gb1 = gW1 + kHidden * kFeatDim;
+  float* gW2 = gb1 + kHidden;
+  float* gb2 = gW2 + kHidden * kHidden;
+  float* gW3 = gb2 + kHidden;
+  float* gb3 = gW3 + kHidden;
+  float lsum = 0.f;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t n_iter = (b.n + stride - 1) / stride;
+  for (uint32_t it = 0; it < n_iter; ++it) {
+    const uint32_t i = it * stride + blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < b.n;   // invalid lanes run with zero error (no contribution)
+    float xn[kFeatDim];
+#pragma unroll
+    for (int f = 0; f < kFeatDim; ++f) {
+      const float x = valid ? b.feats[(size_t)i * kFeatDim + f] : m.in_mean[f];
+      xn[f] = (x - m.in_mean[f]) / m.in_std[f];
+    }
+    float h1[kHidden], h2[kHidden];
+#pragma unroll
+    for (int j = 0; j < kHidden; ++j) {
+      float s = m.b1[j];
+#pragma unroll
+      for (int f = 0; f < kFeatDim; ++f) s = fmaf(m.W1[j * kFeatDim + f], xn[f], s);
+      h1[j] = fmaxf(s, 0.f);
+    }
+    float o = m.b3;
+#pragma unroll
+    for (int j = 0; j < kHidden; ++j) {
+      float s = m.b2[j];
+#pragma unroll
+      for (int k = 0; k < kHidden; ++k) s = fmaf(m.W2[j * kHidden + k], h1[k], s);
+      h2[j] = fmaxf(s, 0.f);
+      o = fmaf(m.W3[j], h2[j], o);
+    }
+    const float tn = valid ? (b.target[i] - m.out_mean) / m.out_std : o;
+    const float err = o - tn;          // d(0.5 err^2)/do
+    lsum += 0.5f * err * err;
+    // output layer
+    float g = warp_sum(err);
+    if (lane == 0) atomicAdd(gb3, g);
+    float dh2[kHidden];
+#pragma unroll
+    for (int j = 0; j < kHidden; ++j) {
+      g = warp_sum(err * h2[j]);
+      if (lane == 0) atomicAdd(&gW3[j], g);
+      dh2[j] = (h2[j] > 0.f) ? err * m.W3[j] : 0.f;
+    }
+    // hidden layer 2
+    float dh1[kHidden];
+#pragma unroll
+    for (int k = 0; k < kHidden; ++k) dh1[k] = 0.f;
+#pragma unroll
+    for (int j = 0; j < kHidden; ++j) {
+      g = warp_sum(dh2[j]);
+      if (lane == 0) atomicAdd(&gb2[j], g);
+#pragma unroll
+      for (int k = 0; k < kHidden; ++k) {
+        g = warp_sum(dh2[j] * h1[k]);
+        if (lane == 0) atomicAdd(&gW2[j * kHidden + k], g);
+        dh1[k] = fmaf(dh2[j], m.W2[j * kHidden + k], dh1[k]);
+      }
+    }
+    // hidden layer 1
+#pragma unroll
+    for (int k = 0; k < kHidden; ++k) {
+      const float d = (h1[k] > 0.f) ? dh1[k] : 0.f;
+      g = warp_sum(d);
+      if (lane == 0) atomicAdd(&gb1[k], g);
+#pragma unroll
+      for (int f = 0; f < kFeatDim; ++f) {
+        g = warp_sum(d * xn[f]);
+        if (lane == 0) atomicAdd(&gW1[k * kFeatDim + f], g);
+      }
+    }
+  }
+  lsum = warp_sum(lsum);
+  if (lane == 0) atomicAdd(loss_sum, lsum);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kTrainParams; i += blockDim.x) atomicAdd(&grad[i], s_g[i]);
+}
+
+__global__ void k_mlp_adam(float* __restrict__ P, const float* __restrict__ grad,
+                           float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                           float b2, float eps, uint32_t step, float scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kTrainParams) return;
+  const float g = grad[i] * scale;
+  const float mi = b1 * m[i] + (1.f - b1) * g;
+  const float vi = b2 * v[i] + (1.f - b2) * g * g;
+  m[i] = mi; v[i] = vi;
+  const float mh = mi / (1.f - powf(b1, (float)step));
+  const float vh = vi / (1.f - powf(b2, (float)step));
+  P[kNormParams + i] -= lr * mh / (sqrtf(vh) + eps);
+}
+
+__global__ void __launch_bounds__(256)
+k_mlp_forward(const float* __restrict__ P, const float* __restrict__ feats, uint32_t n,
+              float* __restrict__ y) {
+  __shared__ float s_p[kModelParams];
+  for (int i = threadIdx.x; i < kModelParams; i += blockDim.x) s_p[i] = P[i];
+  __syncthreads();
+  const MlpView m = mlp_view(s_p);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float x[kFeatDim];
+#pragma unroll
+    for (int f = 0; f < kFeatDim; ++f) x[f] = feats[(size_t)i * kFeatDim + f];
+    y[i] = fmaf(mlp_forward_norm(m, x), m.out_std, m.out_mean);
+  }
+}
+
+// K-th neighbor distance of each query from rows sorted by (distance, index);
+// -1 when the row has fewer than K neighbors.
+__global__ void k_kth_dist(const int32_t* __restrict__ rows, uint32_t nq, uint32_t k,
+                           const float* __restrict__ pts, const float* __restrict__ qs,
+                           float* __restrict__ kth) {
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    const int32_t p = rows[(size_t)q * k + (k - 1)];
+    float d = -1.f;
+    if (p >= 0) {
+      const float* a = qs + 3ull * q;
+      const float* b = pts + 3ull * (uint32_t)p;
+      d = sqrtf(dist2_ref(a[0], a[1], a[2], b[0], b[1], b[2]));
+    }
+    kth[q] = d;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_widths(const WidthArgs& a, int n_sms, cudaStream_t s) {
+  if (a.n_queries == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)min((uint64_t)n_sms * 8, ((uint64_t)a.n_queries + 255) / 256);
+  k_widths<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_loss_grad(const float* params, const MlpBatch& b, float* grad,
+                                 float* loss_sum, int n_sms, cudaStream_t s) {
+  if (b.n == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)min((uint64_t)n_sms * 2, ((uint64_t)b.n + 255) / 256);
+  k_mlp_loss_grad<<<blocks, 256, 0, s>>>(params, b, grad, loss_sum);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_adam(float* params, const float* grad, float* m, float* v, float lr,
+                            float beta1, float beta2, float eps, uint32_t step, float scale,
+                            cudaStream_t s) {
+  k_mlp_adam<<<(kTrainParams + 255) / 256, 256, 0, s>>>(params, grad, m, v, lr, beta1, beta2,
+                                                         eps, step, scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_forward(const float* params, const float* feats, uint32_t n, float* y,
+                               int n_sms, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)min((uint64_t)n_sms * 8, ((uint64_t)n + 255) / 256);
+  k_mlp_forward<<<blocks, 256, 0, s>>>(params, feats, n, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kth_dist(const int32_t* rows, uint32_t n_queries, uint32_t k,
+                            const float* points, const float* queries, float* kth_d,
+                            cudaStream_t s) {
+  if (n_queries == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)min(4096u, (n_queries + 255) / 256);
+  k_kth_dist<<<blocks, 256, 0, s>>>(rows, n_queries, k, points, queries, kth_d);
+  return cudaGetLastError();
+}
+
+}  // namespace rtnn

@@ -1,0 +1,132 @@
+// radix_sort.cu -- stable LSD radix sort of (key, uint32 value) pairs, 8-bit digits.
+//
+// Replaces the CUB radix sorts behind thrust::sort_by_key in the reference
+// (thrust_helper.cu:13-43; call sites sort.cpp:415,487-488,612). Used to put queries
+// in Morton order. Each pass: (1) per-tile digit histograms, column-major
+// [digit][tile]; (2) one exclusive scan of that table (scan.cu), giving every
+// (digit, tile) its global output offset; (3) a stable scatter: each warp ranks its
+// 512-key sub-tile with __match_any_sync, warps are combined through a shared-memory
+// prefix per digit, and keys keep their input order within a digit.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rtnn {
+namespace {
+
+constexpr int kWarps = kRadixThreads / 32;
+constexpr int kSub = 32 * kRadixItems;   // keys per warp sub-tile
+
+template <typename KeyT>
+__global__ void __launch_bounds__(kRadixThreads)
+k_radix_hist(const KeyT* __restrict__ keys, uint32_t n, uint32_t shift,
+             uint32_t* __restrict__ hist, uint32_t n_tiles) {
+  __shared__ uint32_t s_h[kWarps][256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < kWarps * 256; i += blockDim.x) (&s_h[0][0])[i] = 0u;
+  __syncthreads();
+  const uint32_t base = blockIdx.x * (uint32_t)kRadixTile + warp * kSub;
+#pragma unroll 4
+  for (int it = 0; it < kRadixItems; ++it) {
+    const uint32_t i = base + it * 32 + lane;
+    if (i < n) atomicAdd(&s_h[warp][(uint32_t)(keys[i] >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) s += s_h[w][d];
+    hist[(uint64_t)d * n_tiles + blockIdx.x] = s;
+  }
+}
+
+template <typename KeyT>
+__global__ void __launch_bounds__(kRadixThreads)
+k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                KeyT* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
+                uint32_t shift, const uint32_t* __restrict__ offsets, uint32_t n_tiles) {
+  __shared__ uint32_t s_cnt[kWarps][256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < kWarps * 256; i += blockDim.x) (&s_cnt[0][0])[i] = 0u;
+  __syncthreads();
+  const uint32_t base = blockIdx.x * (uint32_t)kRadixTile + warp * kSub;
+  KeyT k[kRadixItems];
+  uint32_t v[kRadixItems], rk[kRadixItems];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int it = 0; it < kRadixItems; ++it) {
+    const uint32_t i = base + it * 32 + lane;
+    const bool valid = i < n;
+    k[it] = valid ? keys_in[i] : (KeyT)0;
+    v[it] = valid ? (vals_in ? vals_in[i] : i) : 0u;
+    const uint32_t digit = valid ? ((uint32_t)(k[it] >> shift) & 0xffu) : 256u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, digit);
+    uint32_t before = 0;
+    if (valid) before = s_cnt[warp][digit];
+    __syncwarp();
+    rk[it] = before + __popc(peers & lt);
+    if (valid && (peers & lt) == 0) s_cnt[warp][digit] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: global offset of this tile, then the warps in order
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+    uint32_t run = offsets[(uint64_t)d * n_tiles + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = s_cnt[w][d];
+      s_cnt[w][d] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < kRadixItems; ++it) {
+    const uint32_t i = base + it * 32 + lane;
+    if (i < n) {
+      const uint32_t digit = (uint32_t)(k[it] >> shift) & 0xffu;
+      const uint32_t dst = s_cnt[warp][digit] + rk[it];
+      keys_out[dst] = k[it];
+      vals_out[dst] = v[it];
+    }
+  }
+}
+
+}  // namespace
+
+uint32_t radix_tiles_for(uint64_t n) { return (uint32_t)((n + kRadixTile - 1) / kRadixTile); }
+
+// Sorts n pairs on bits [0, bits). Ping-pongs between (keys0, vals0) and (keys1, vals1);
+// *result_in_1 tells where the sorted pairs ended up. identity_values: the first pass
+// reads value i for position i instead of vals0.
+cudaError_t radix_sort_pairs(bool key64, void* keys0, uint32_t* vals0, void* keys1,
+                             uint32_t* vals1, uint32_t n, uint32_t bits, bool identity_values,
+                             uint32_t* hist, uint64_t* scan_state, uint32_t* scan_counters,
+                             Counters* ctr, bool* result_in_1, cudaStream_t s) {
+  *result_in_1 = false;
+  if (n == 0) return cudaSuccess;
+  const uint32_t n_tiles = radix_tiles_for(n);
+  const uint32_t passes = (bits + 7) / 8;
+  bool in1 = false;
+  cudaError_t e = cudaSuccess;
+  for (uint32_t p = 0; p < passes; ++p) {
+    void* kin = in1 ? keys1 : keys0;
+    void* kout = in1 ? keys0 : keys1;
+    const uint32_t* vin = (p == 0 && identity_values) ? nullptr : (in1 ? vals1 : vals0);
+    uint32_t* vout = in1 ? vals0 : vals1;
+    const uint32_t shift = 8 * p;
+    if (key64) k_radix_hist<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint64_t*)kin, n, shift, hist, n_tiles);
+    else k_radix_hist<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint32_t*)kin, n, shift, hist, n_tiles);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const uint64_t hn = 256ull * n_tiles;
+    e = launch_scan_excl(hist, hn, nullptr, 0, hn, scan_state, scan_counters + p, ctr, s);
+    if (e != cudaSuccess) return e;
+    if (key64) k_radix_scatter<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint64_t*)kin, vin, (uint64_t*)kout, vout, n, shift, hist, n_tiles);
+    else k_radix_scatter<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint32_t*)kin, vin, (uint32_t*)kout, vout, n, shift, hist, n_tiles);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    in1 = !in1;
+  }
+  *result_in_1 = in1;
+  return cudaSuccess;
+}
+
+}  // namespace rtnn

@@ -1,0 +1,273 @@
+// search.cu -- warp-cooperative cell-walk search (fixed-radius and KNN).
+//
+// Replaces the OptiX traversal of the reference: __raygen__radius / __raygen__knn
+// (camera.cu:39-146) launching one zero-length ray per query, and the intersection
+// programs __intersection__sphere_radius / __intersection__sphere_knn with
+// check_intersect, write_res_radius and insertTopKQ (geometry.cu:38-191).
+//
+// Work item = a tile of 32 Morton-ordered queries of one cloud, handled by one warp;
+// a persistent grid pulls tiles from an atomic counter. Per tile:
+//   1. the warp reduces the tiles's bounding box and widest search width R;
+//   2. the candidate cells are the grid box covering bbox +- R; in raster order each
+//      (y, z) row of that box is one contiguous range of the cell-sorted points, so a
+//      row costs two offset loads (computed lane-parallel, 32 rows at a time);
+//   3. each range is streamed 32 points at a time with 16-byte loads, the points farther
+//      than R from the tile box are dropped, and the survivors are compacted with
+//      __ballot_sync into a per-warp shared-memory stage;
+//   4. every lane tests every staged point against its own query with the reference's
+//      FP32 distance (common.cuh: dist2_ref) and keeps its K smallest (distance, index)
+//      pairs in a max-heap in shared memory ([slot][lane], conflict-free columns);
+//   5. rows are written warp-cooperatively (coalesced), unused slots = -1.
+// Queries whose search width was narrowed by the partition (width < r) and that found
+// fewer than K neighbors inside it are appended to a fallback list; a second pass of
+// this kernel re-searches them at the full radius, so every row is exact.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rtnn {
+namespace {
+
+__device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t i, uint32_t k, uint64_t x) {
+  while (true) {
+    uint32_t c = 2 * i + 1;
+    if (c >= k) break;
+    uint64_t cv = h[c * 32];
+    if (c + 1 < k) {
+      const uint64_t c2 = h[(c + 1) * 32];
+      if (c2 > cv) { cv = c2; ++c; }
+    }
+    if (cv <= x) break;
+    h[i * 32] = cv;
+    i = c;
+  }
+  h[i * 32] = x;
+}
+
+__device__ __forceinline__ float wmin(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float wmax(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <bool KNN>
+__global__ void __launch_bounds__(256)
+k_search(SearchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  float4* stage = reinterpret_cast<float4*>(smem) + warp * 32;
+  uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * 512) + (size_t)warp * a.k * 32;
+  uint64_t* heap = heapw + lane;   // this lane's column: heap[i * 32]
+  const uint32_t lt = lanemask_lt();
+  const uint32_t k = a.k;
+  const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
+  const bool local_idx = (a.flags & kSearchLocalIndices) != 0;
+  const uint32_t fb_total = a.fallback_pass ? a.ctr->fb_count : 0u;
+  const uint32_t n_tiles = a.fallback_pass ? (fb_total + 31) / 32 : a.n_tiles;
+  const uint32_t total_cells = a.ctr->total_cells;
+
+  while (true) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.work, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= n_tiles) break;
+
+    bool valid;
+    uint32_t pos, cloud;
+    if (!a.fallback_pass) {
+      uint32_t c = 0;
+      if (lane == 0) c = find_cloud(a.t.tile_base, a.t.n_clouds, tile);
+      cloud = __shfl_sync(0xffffffffu, c, 0);
+      const uint32_t q0 = a.t.query_off[cloud] + (tile - a.t.tile_base[cloud]) * 32u;
+      pos = q0 + lane;
+      valid = pos < a.t.query_off[cloud + 1];
+    } else {
+      const uint32_t e = tile * 32u + lane;
+      valid = e < fb_total;
+      pos = valid ? a.fb_pos[e] : 0u;
+      cloud = valid ? a.fb_cloud[e] : 0u;
+    }
+    float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float w = a.radius, lim = a.r2;
+    if (valid && !a.fallback_pass && a.qwidth) {
+      const float wq = a.qwidth[pos];
+      if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
+    }
+    valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
+
+    uint32_t pending = __ballot_sync(0xffffffffu, valid);
+    while (pending) {
+      const int leader = __ffs(pending) - 1;
+      const uint32_t gcloud = __shfl_sync(0xffffffffu, cloud, leader);
+      const uint32_t group = __ballot_sync(0xffffffffu, valid && cloud == gcloud) & pending;
+      pending &= ~group;
+      const bool act = (group >> lane) & 1u;
+
+      // 1. group bounding box and widest width
+      const float bx0 = wmin(act ? q.x : INFINITY), bx1 = wmax(act ? q.x : -INFINITY);
+      const float by0 = wmin(act ? q.y : INFINITY), by1 = wmax(act ? q.y : -INFINITY);
+      const float bz0 = wmin(act ? q.z : INFINITY), bz1 = wmax(act ? q.z : -INFINITY);
+      // widen by 2^-20 relative: covers every point whose rounded FP32 distance passes
+      const float R = __fmul_ru(wmax(act ? w : 0.f), 1.000001f);
+      const float Rk = __fmul_ru(R, 1.0001f);
+      const float R2k = __fmul_ru(Rk, Rk);
+      const CloudGrid g = a.grids[gcloud];
+      // a grid that overran the cell array (reported by the plan) is never read
+      const bool grid_ok = (uint64_t)g.cell_base + g.n_cells <= (uint64_t)total_cells;
+
+      // 2. candidate cell box
+      const float fx0 = cell_coord_f(__fsub_rn(bx0, R), g.ox, g.inv_cell);
+      const float fx1 = cell_coord_f(__fadd_rn(bx1, R), g.ox, g.inv_cell);
+      const float fy0 = cell_coord_f(__fsub_rn(by0, R), g.oy, g.inv_cell);
+      const float fy1 = cell_coord_f(__fadd_rn(by1, R), g.oy, g.inv_cell);
+      const float fz0 = cell_coord_f(__fsub_rn(bz0, R), g.oz, g.inv_cell);
+      const float fz1 = cell_coord_f(__fadd_rn(bz1, R), g.oz, g.inv_cell);
+      const bool empty = !(grid_ok && fx0 <= (float)(g.dx - 1) && fx1 >= 0.f &&
+                           fy0 <= (float)(g.dy - 1) && fy1 >= 0.f && fz0 <= (float)(g.dz - 1) &&
+                           fz1 >= 0.f);
+      const int lx = (int)fmaxf(fx0, 0.f), hx = (int)fminf(fx1, (float)(g.dx - 1));
+      const int ly = (int)fmaxf(fy0, 0.f), hy = (int)fminf(fy1, (float)(g.dy - 1));
+      const int lz = (int)fmaxf(fz0, 0.f), hz = (int)fminf(fz1, (float)(g.dz - 1));
+      const int ny = hy - ly + 1, nz = hz - lz + 1;
+      const int nrows = empty ? 0 : ny * nz;
+
+      const float lim_l = act ? lim : -1.f;
+      uint32_t n = 0;
+      uint64_t root = ~0ull;
+      float root_d = INFINITY;
+
+      for (int rb = 0; rb < nrows; rb += 32) {
+        uint32_t rs = 0, re = 0;
+        const int ri = rb + lane;
+        if (ri < nrows) {
+          const int cy = ly + ri % ny, cz = lz + ri / ny;
+          const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+          rs = __ldg(a.cells + rowc + lx);
+          re = __ldg(a.cells + rowc + hx + 1);
+        }
+        const int nr = min(32, nrows - rb);
+        for (int j = 0; j < nr; ++j) {
+          const uint32_t s0 = __shfl_sync(0xffffffffu, rs, j);
+          const uint32_t e0 = __shfl_sync(0xffffffffu, re, j);
+          for (uint32_t b = s0; b < e0; b += 32) {
+            // 3. stream 32 points, drop those farther than R from the box, compact
+            const uint32_t idx = b + lane;
+            bool keep = false;
+            float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (idx < e0) {
+              p = __ldg(a.spts + idx);
+              const float ex = fmaxf(fmaxf(bx0 - p.x, p.x - bx1), 0.f);
+              const float ey = fmaxf(fmaxf(by0 - p.y, p.y - by1), 0.f);
+              const float ez = fmaxf(fmaxf(bz0 - p.z, p.z - bz1), 0.f);
+              keep = ex * ex + ey * ey + ez * ez <= R2k;
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            if (keep) stage[__popc(m & lt)] = p;
+            __syncwarp();
+            const int cnt = __popc(m);
+            // 4. every lane against every staged point
+            for (int c = 0; c < cnt; ++c) {
+              const float4 cp = stage[c];
+              const float d = dist2_ref(q.x, q.y, q.z, cp.x, cp.y, cp.z);
+              const bool hit = (d < lim_l) && (!KNN || d > 0.f) && (d <= root_d);
+              if (hit) {
+                const uint64_t key = ((uint64_t)__float_as_uint(d) << 32) | __float_as_uint(cp.w);
+                if (n < k) {
+                  heap[n * 32] = key;
+                  ++n;
+                  if (n == k) {
+                    for (int i = (int)k / 2 - 1; i >= 0; --i) heap_sift_down(heap, i, k, heap[i * 32]);
+                    root = heap[0];
+                    root_d = __uint_as_float((uint32_t)(root >> 32));
+                  }
+                } else if (key < root) {
+                  heap_sift_down(heap, 0, k, key);
+                  root = heap[0];
+                  root_d = __uint_as_float((uint32_t)(root >> 32));
+                }
+              }
+            }
+            __syncwarp();
+          }
+        }
+      }
+
+      // completion: a narrowed search that found fewer than K neighbors is redone at r
+      const bool incomplete = act && (lim_l < a.r2) && (n < k);
+      const bool done = act && !incomplete;
+      const uint32_t fbm = __ballot_sync(0xffffffffu, incomplete);
+      if (fbm) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&a.ctr->fb_count, (uint32_t)__popc(fbm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (incomplete) {
+          const uint32_t e = base + __popc(fbm & lt);
+          a.fb_out_pos[e] = pos;
+          a.fb_out_cloud[e] = gcloud;
+        }
+      }
+      if (done && sorted_rows) {
+        for (uint32_t i = 1; i < n; ++i) {
+          const uint64_t x = heap[i * 32];
+          uint32_t j = i;
+          while (j > 0 && heap[(j - 1) * 32] > x) { heap[j * 32] = heap[(j - 1) * 32]; --j; }
+          heap[j * 32] = x;
+        }
+      }
+      __syncwarp();
+      // 5. coalesced row writes
+      const uint32_t sub = local_idx ? a.t.point_off[gcloud] : 0u;
+      uint32_t wm = __ballot_sync(0xffffffffu, done);
+      while (wm) {
+        const int L = __ffs(wm) - 1;
+        wm &= wm - 1;
+        const uint32_t nL = __shfl_sync(0xffffffffu, n, L);
+        const uint32_t qi = __float_as_uint(__shfl_sync(0xffffffffu, q.w, L));
+        int32_t* row = a.out + (size_t)qi * k;
+        for (uint32_t jj = lane; jj < k; jj += 32) {
+          int32_t v = -1;
+          if (jj < nL) v = (int32_t)((uint32_t)heapw[jj * 32 + L] - sub);
+          row[jj] = v;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+}  // namespace
+
+size_t search_smem_bytes(uint32_t k, int warps_per_block) {
+  return (size_t)warps_per_block * (512 + (size_t)k * 32 * 8);
+}
+
+cudaError_t search_prepare(int device) {
+  (void)device;
+  cudaError_t e = cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  return e;
+}
+
+int search_blocks_per_sm(bool knn, uint32_t k, int warps_per_block) {
+  int nb = 0;
+  const size_t smem = search_smem_bytes(k, warps_per_block);
+  cudaError_t e = knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<true>, warps_per_block * 32, smem)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<false>, warps_per_block * 32, smem);
+  if (e != cudaSuccess) return 1;
+  return nb > 0 ? nb : 1;
+}
+
+cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
+                          cudaStream_t s) {
+  const size_t smem = search_smem_bytes(a.k, warps_per_block);
+  if (knn) k_search<true><<<blocks, warps_per_block * 32, smem, s>>>(a);
+  else k_search<false><<<blocks, warps_per_block * 32, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace rtnn

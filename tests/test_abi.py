@@ -1,0 +1,81 @@
+"""C-ABI library: loads, exports every declared symbol, rejects bad calls (CPU only)."""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+import rtnn_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*[A-Za-z_][\w \*]*?\b(rtnn_\w+)\s*\(", src, flags=re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(rtnn_b200.library_path())
+    names = _declared()
+    assert "rtnn_search" in names and "rtnn_search_batched" in names
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_mirror_binds_every_declared_symbol():
+    lib = rtnn_b200.load_library()
+    for n in _declared():
+        assert n in rtnn_b200._SIGS, f"{n} has no Python binding"
+        assert getattr(lib, n).argtypes is not None
+
+
+def test_version_and_k_range():
+    lib = rtnn_b200.load_library()
+    assert b"sm_100a" in lib.rtnn_version()
+    assert lib.rtnn_k_supported(1) == 1 and lib.rtnn_k_supported(rtnn_b200.MAX_K) == 1
+    assert lib.rtnn_k_supported(0) == 0 and lib.rtnn_k_supported(rtnn_b200.MAX_K + 1) == 0
+
+
+def test_model_size_matches_layout():
+    lib = rtnn_b200.load_library()
+    F, H = 6, 32
+    assert lib.rtnn_model_size() == 2 * F + 2 + H * F + H + H * H + H + H + 1
+
+
+def _have_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_have_gpu(), reason="checks the no-device error path")
+def test_create_without_device_reports_no_device():
+    with pytest.raises(rtnn_b200.RtnnError) as e:
+        rtnn_b200.Context(0)
+    assert e.value.code == "RTNN_ERR_NO_DEVICE"
+
+
+def test_null_context_is_rejected():
+    lib = rtnn_b200.load_library()
+    out = np.zeros(4, dtype=np.int32)
+    st = lib.rtnn_search(None, None, 0, None, 0, 0, 1.0, 1, 0, out.ctypes.data_as(ctypes.c_void_p), None)
+    assert st == 1  # RTNN_ERR_INVALID_ARGUMENT
+    assert lib.rtnn_destroy(None) == 0
+    assert lib.rtnn_plan_destroy(None) == 0
+
+
+def test_mode_names():
+    assert rtnn_b200._mode("radius") == rtnn_b200.RADIUS
+    assert rtnn_b200._mode("knn") == rtnn_b200.KNN
+    with pytest.raises(ValueError):
+        rtnn_b200._mode("nearest")

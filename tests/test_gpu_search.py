@@ -1,0 +1,269 @@
+"""Parity of the CUDA search (through the C ABI) with the oracle -- needs a B200.
+
+Index work is compared bit-exactly: each row's neighbor set equals the oracle's, and
+with sorted rows the row itself equals the oracle row (order by (FP32 distance, index)).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import rtnn_b200
+from rtnn_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+BIG = np.iinfo(np.int32).max
+
+
+def as_sets(rows):
+    """Rows with their valid entries sorted ascending and -1 kept last."""
+    r = np.where(rows < 0, BIG, rows)
+    r = np.sort(r, axis=1)
+    return np.where(r == BIG, -1, r)
+
+
+def assert_rows_equal(got, exp, sorted_rows):
+    assert got.shape == exp.shape
+    if sorted_rows:
+        bad = np.nonzero((got != exp).any(1))[0]
+    else:
+        bad = np.nonzero((as_sets(got) != as_sets(exp)).any(1))[0]
+    assert bad.size == 0, f"{bad.size} rows differ, first {bad[:5].tolist()}: got {got[bad[0]].tolist()} exp {exp[bad[0]].tolist()}"
+    # every row: the valid entries come first, then only -1
+    valid = got >= 0
+    assert (valid[:, :-1] | ~valid[:, 1:]).all()
+
+
+def test_samplepc_golden(ctx):
+    with open(os.path.join(GOLDEN, "samplepc.json")) as f:
+        g = json.load(f)
+    pts = np.asarray(g["points"], dtype=np.float32)
+    for run in g["runs"]:
+        got = ctx.search(pts, None, run["mode"], run["radius"], run["k"], sorted_rows=True)
+        assert got.tolist() == run["rows"]
+
+
+@pytest.mark.parametrize("sorted_rows", [False, True])
+def test_uniform_radius_full_config(ctx, sorted_rows):
+    """Plain fixed-radius search, N = Q = 100,000 uniform in [0,100]^3, r = 4, K = 50."""
+    p = wl.uniform_cube(100_000, 100.0, seed=0)
+    st = rtnn_b200.Stats()
+    got = ctx.search(p, None, "radius", 4.0, 50, sorted_rows=sorted_rows, stats=st)
+    exp = oracle.grid_search(p, None, "radius", 4.0, 50)
+    assert_rows_equal(got, exp, sorted_rows)
+    assert st.n_fallback == 0 and st.n_queries == 100_000
+
+
+def test_uniform_radius_reference_check(ctx):
+    p = wl.uniform_cube(20_000, 60.0, seed=5)
+    got = ctx.search(p, None, "radius", 4.0, 50)
+    ok, log = oracle.refcheck(p, None, got, "radius", 4.0, 50)
+    assert ok, log
+    got = ctx.search(p, None, "knn", 4.0, 8)
+    ok, log = oracle.refcheck(p, None, got, "knn", 4.0, 8, 0, 2000)
+    assert ok, log
+
+
+@pytest.mark.parametrize("flags", [{}, {"partition": True}])
+def test_gmm_knn_small(ctx, flags):
+    """KNN K=5, r=10 on a Gaussian mixture with separate uniform queries (scaled)."""
+    p, q = wl.gmm(scale=0.05, seed=1)
+    got = ctx.search(p, q, "knn", 10.0, 5, sorted_rows=True, **flags)
+    exp = oracle.grid_search(p, q, "knn", 10.0, 5)
+    assert_rows_equal(got, exp, True)
+
+
+def test_gmm_knn_full_size_subset(ctx):
+    """Full-size KNN config (1e6 points, 1e6 queries): plain and partitioned runs agree
+    everywhere, and a seeded subset of rows matches the oracle's brute force."""
+    p, q = wl.gmm(seed=1)
+    a = ctx.search(p, q, "knn", 10.0, 5, sorted_rows=True)
+    st = rtnn_b200.Stats()
+    b = ctx.search(p, q, "knn", 10.0, 5, sorted_rows=True, partition=True, stats=st)
+    assert np.array_equal(a, b)
+    assert st.n_fallback < q.shape[0]
+    idx = np.random.default_rng(0).choice(q.shape[0], 1000, replace=False)
+    exp = oracle.bruteforce(p, q[idx], "knn", 10.0, 5)
+    assert np.array_equal(a[idx], exp)
+
+
+@pytest.mark.parametrize("mode,r,k", [("knn", 2.0, 16), ("radius", 2.0, 16)])
+def test_surfaces_partition(ctx, mode, r, k):
+    p = wl.surfaces(scale=0.01, seed=2)
+    exp = oracle.grid_search(p, None, mode, r, k)
+    for kw in ({}, {"partition": True}):
+        st = rtnn_b200.Stats()
+        got = ctx.search(p, None, mode, r, k, stats=st, **kw)
+        assert_rows_equal(got, exp, False)
+
+
+def test_sph_lattice_radius_k64(ctx):
+    p = wl.sph_lattice(scale=0.0005, seed=4)
+    p = wl.sph_step(p, seed=1)
+    got = ctx.search(p, None, "radius", 2.0, 64, partition=True)
+    exp = oracle.grid_search(p, None, "radius", 2.0, 64)
+    assert_rows_equal(got, exp, False)
+
+
+@pytest.mark.parametrize("k", [1, 2, 31, 32, 33, 64, 100, 128])
+def test_k_range(ctx, k):
+    p = wl.uniform_cube(8000, 20.0, seed=k)
+    for mode in ("radius", "knn"):
+        got = ctx.search(p, None, mode, 2.5, k, sorted_rows=True)
+        exp = oracle.grid_search(p, None, mode, 2.5, k)
+        assert_rows_equal(got, exp, True)
+
+
+def test_lattice_ties_break_by_index(ctx):
+    g = np.stack(np.meshgrid(np.arange(12), np.arange(12), np.arange(12), indexing="ij"), -1)
+    p = g.reshape(-1, 3).astype(np.float32)
+    for mode, r, k in (("knn", 1.5, 4), ("knn", 2.0, 10), ("radius", 1.5, 5), ("radius", 1.0001, 3)):
+        got = ctx.search(p, None, mode, r, k, sorted_rows=True)
+        exp = oracle.bruteforce(p, None, mode, r, k)
+        assert_rows_equal(got, exp, True)
+
+
+def test_points_exactly_at_radius_are_excluded(ctx):
+    p = np.array([[0, 0, 0], [2, 0, 0], [0, 2, 0], [1.9999999, 0, 0], [0, 0, -2]], np.float32)
+    got = ctx.search(p, None, "radius", 2.0, 8, sorted_rows=True)
+    exp = oracle.bruteforce(p, None, "radius", 2.0, 8)
+    assert_rows_equal(got, exp, True)
+    assert 1 not in got[0] and 3 in got[0]
+
+
+def test_duplicates(ctx):
+    p = np.zeros((300, 3), np.float32)
+    p[200:] = 0.5
+    knn = ctx.search(p, None, "knn", 1.0, 8)
+    # coincident points are excluded in KNN: the 200 zeros only see the 100 halves
+    assert (knn[:200] >= 200).all()
+    rad = ctx.search(p, None, "radius", 1.0, 8, sorted_rows=True)
+    exp = oracle.bruteforce(p, None, "radius", 1.0, 8)
+    assert_rows_equal(rad, exp, True)
+
+
+def test_empty_inputs(ctx):
+    p = wl.uniform_cube(100, 10.0, seed=1)
+    empty = np.zeros((0, 3), np.float32)
+    out = ctx.search(empty, p, "radius", 1.0, 4)
+    assert out.shape == (100, 4) and (out == -1).all()
+    out = ctx.search(p, empty, "knn", 1.0, 4)
+    assert out.shape == (0, 4)
+
+
+def test_far_and_nonfinite_queries(ctx):
+    p = wl.uniform_cube(2000, 10.0, seed=2)
+    q = np.array([[1e6, 1e6, 1e6], [-1e30, 0, 0], [np.nan, 1, 1], [np.inf, 0, 0], [5, 5, 5]],
+                 np.float32)
+    got = ctx.search(p, q, "knn", 2.0, 6, sorted_rows=True)
+    assert (got[:4] == -1).all()
+    exp = oracle.bruteforce(p, q[4:], "knn", 2.0, 6)
+    assert np.array_equal(got[4:], exp)
+
+
+def test_invalid_arguments(ctx):
+    p = wl.uniform_cube(10, 1.0, seed=0)
+    with pytest.raises(rtnn_b200.RtnnError) as e:
+        ctx.search(p, None, "knn", 1.0, 0)
+    assert e.value.code == "RTNN_ERR_UNSUPPORTED_K"
+    with pytest.raises(rtnn_b200.RtnnError) as e:
+        ctx.search(p, None, "knn", 1.0, 129)
+    assert e.value.code == "RTNN_ERR_UNSUPPORTED_K"
+    for bad_r in (0.0, -1.0, float("nan"), float("inf")):
+        with pytest.raises(rtnn_b200.RtnnError) as e:
+            ctx.search(p, None, "radius", bad_r, 4)
+        assert e.value.code == "RTNN_ERR_INVALID_ARGUMENT"
+    fresh = rtnn_b200.Context(0)
+    with pytest.raises(rtnn_b200.RtnnError) as e:
+        fresh.search(p, None, "knn", 1.0, 4, learned=True)
+    assert e.value.code == "RTNN_ERR_NO_MODEL"
+    fresh.close()
+    # the context stays usable after rejected calls
+    assert ctx.search(p, None, "radius", 1.0, 4).shape == (10, 4)
+
+
+def test_device_pointers(ctx):
+    import torch
+    p, q = wl.gmm(scale=0.02, seed=7)
+    tp = torch.from_numpy(p).cuda()
+    tq = torch.from_numpy(q).cuda()
+    out = ctx.search(tp, tq, "knn", 10.0, 5, sorted_rows=True)
+    assert out.is_cuda and out.dtype == torch.int32
+    exp = oracle.grid_search(p, q, "knn", 10.0, 5)
+    assert np.array_equal(out.cpu().numpy(), exp)
+
+
+def test_unaligned_inputs(ctx):
+    """Inputs starting off a 16-byte boundary take the scalar load path."""
+    import torch
+    p = wl.uniform_cube(5001, 20.0, seed=3)
+    buf = torch.from_numpy(np.concatenate([np.zeros(1, np.float32), p.ravel()])).cuda()
+    tp = buf[1:].view(-1, 3)
+    assert tp.data_ptr() % 16 != 0
+    out = ctx.search(tp, None, "radius", 2.0, 12, sorted_rows=True)
+    exp = oracle.grid_search(p, None, "radius", 2.0, 12)
+    assert np.array_equal(out.cpu().numpy(), exp)
+
+
+def test_batched_matches_per_cloud_oracle(ctx):
+    p, off = wl.multicloud(n_clouds=64, lo=16, hi=4000, seed=3)
+    for local in (False, True):
+        st = rtnn_b200.Stats()
+        got = ctx.search_batched(p, off, mode="knn", radius=0.2, k=32, local_indices=local,
+                                 stats=st)
+        exp = oracle.grid_search_batched(p, off, mode="knn", r=0.2, k=32, local=local)
+        assert_rows_equal(got, exp, False)
+        assert st.n_clouds == 64
+
+
+def test_batched_separate_queries_and_empty_clouds(ctx):
+    rng = np.random.default_rng(8)
+    psz = [100, 0, 50, 300, 1]
+    qsz = [20, 5, 0, 40, 3]
+    po = np.concatenate([[0], np.cumsum(psz)]).astype(np.uint64)
+    qo = np.concatenate([[0], np.cumsum(qsz)]).astype(np.uint64)
+    p = rng.uniform(0, 1, (int(po[-1]), 3)).astype(np.float32)
+    q = rng.uniform(0, 1, (int(qo[-1]), 3)).astype(np.float32)
+    for mode in ("knn", "radius"):
+        got = ctx.search_batched(p, po, q, qo, mode=mode, radius=0.3, k=7, partition=True)
+        exp = oracle.grid_search_batched(p, po, q, qo, mode=mode, r=0.3, k=7)
+        assert_rows_equal(got, exp, False)
+
+
+def test_plan_graph_replay(ctx):
+    import torch
+    p, off = wl.multicloud(n_clouds=32, lo=64, hi=3000, seed=5)
+    tp = torch.from_numpy(p).cuda()
+    exp = oracle.grid_search_batched(p, off, mode="knn", r=0.2, k=16)
+    for use_graph in (False, True):
+        plan = ctx.plan(off, mode="knn", radius=0.2, k=16, use_graph=use_graph)
+        for _ in range(3):
+            out = plan.execute(tp)
+            assert_rows_equal(out.cpu().numpy(), exp, False)
+        # new point data of the same shape through the same graph
+        p2 = (p * np.float32(0.9) + np.float32(0.05)).astype(np.float32)
+        tp.copy_(torch.from_numpy(p2))
+        out = plan.execute(tp)
+        exp2 = oracle.grid_search_batched(p2, off, mode="knn", r=0.2, k=16)
+        assert_rows_equal(out.cpu().numpy(), exp2, False)
+        tp.copy_(torch.from_numpy(p))
+        plan.close()
+
+
+def test_fp64_disagreement_is_only_boundary_pairs(ctx):
+    rng = np.random.default_rng(9)
+    p = (rng.integers(0, 40, (3000, 3)) * 0.25).astype(np.float32)
+    for mode, r in (("radius", 1.0), ("knn", 1.25)):
+        got = ctx.search(p, None, mode, r, 128)
+        ref64 = oracle.bruteforce_fp64(p, None, mode, r, 128)
+        pairs = {tuple(v) for v in oracle.boundary_pairs(p, None, mode, r).tolist()}
+        diff = set()
+        for qi in range(p.shape[0]):
+            a = set(got[qi][got[qi] >= 0].tolist())
+            b = set(ref64[qi][ref64[qi] >= 0].tolist())
+            diff |= {(qi, x) for x in a ^ b}
+        assert diff == pairs
