@@ -144,11 +144,17 @@ rtnn_status rtnn_plan_destroy(rtnn_plan* plan);
 
 /* Search-tuning knobs chosen by the autotuner (rtnn_b200/autotune.py caches them). */
 typedef struct rtnn_tuning {
-  float cell_ratio;      /* cell edge = radius * cell_ratio (reference: 1/crRatio, sort.cpp:80) */
-  float cell_budget;     /* max grid cells per point before the cell edge is grown */
-  uint32_t warps_per_block;   /* search kernel block size in warps */
-  uint32_t blocks_per_sm;     /* persistent search grid = SMs * blocks_per_sm */
-  float width_margin;    /* learned width = margin * predicted K-th distance */
+  float cell_ratio;       /* largest cell edge = radius * cell_ratio
+                             (the reference's cellSize = radius / crRatio, sort.cpp:80) */
+  float min_cell_ratio;   /* smallest cell edge = radius * min_cell_ratio */
+  float points_per_cell;  /* > 0: a cloud's cell edge shrinks (down to the smallest) until
+                             its bounding box holds about this many points per cell */
+  float cell_budget;      /* max grid cells per point before the cell edge is grown */
+  uint32_t warps_per_block;   /* search kernel block size in warps (1..8) */
+  uint32_t blocks_per_sm;     /* persistent search grid = SMs * blocks_per_sm (0: occupancy) */
+  float width_margin;     /* learned width = margin * predicted K-th distance */
+  uint32_t fallback_passes;   /* partitioned search: passes that retry short queries at twice
+                                 their width before the last pass at the full radius (0..6) */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

@@ -65,9 +65,10 @@ class Stats(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("cell_ratio", ctypes.c_float), ("cell_budget", ctypes.c_float),
+    _fields_ = [("cell_ratio", ctypes.c_float), ("min_cell_ratio", ctypes.c_float),
+                ("points_per_cell", ctypes.c_float), ("cell_budget", ctypes.c_float),
                 ("warps_per_block", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
-                ("width_margin", ctypes.c_float)]
+                ("width_margin", ctypes.c_float), ("fallback_passes", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

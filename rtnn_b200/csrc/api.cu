@@ -54,11 +54,13 @@ void release(DevBuf& b) {
 }
 
 struct Workspace {
-  DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth, fbpos,
-      fbcloud, hist, scan_state, counters, in_pts, in_qs, out, feats, cellsz, kth;
+  DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth,
+      fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters, in_pts, in_qs, out, feats,
+      cellsz, kth;
   void release_all() {
     for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
-                      &vals1, &sq, &qwidth, &fbpos, &fbcloud, &hist, &scan_state, &counters,
+                      &vals1, &sq, &qwidth, &fbpos[0], &fbpos[1], &fbcloud[0], &fbcloud[1],
+                      &fbwidth[0], &fbwidth[1], &hist, &scan_state, &counters,
                       &in_pts, &in_qs, &out, &feats, &cellsz, &kth})
       release(*b);
   }
@@ -82,6 +84,7 @@ struct Params {
   float radius;
   uint32_t k;
   uint32_t flags;
+  uint32_t fb_passes;   // escalating fallback passes (partitioned searches)
 };
 
 uint32_t ceil_log2(uint64_t x) {
@@ -98,7 +101,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 16.f, 4u, 0u, 1.25f};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
@@ -236,6 +239,8 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
 
 bool partitioned(const Params& p) { return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0; }
 
+uint32_t fallback_passes_of(const Params& p) { return p.fb_passes; }
+
 rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr) {
   const uint64_t n1 = sh.n_clouds + 1ull;
   const uint64_t N = std::max<uint64_t>(sh.N, 1), Q = std::max<uint64_t>(sh.Q, 1);
@@ -254,8 +259,11 @@ rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& 
   RTNN_CU(ensure(ws.sq, Q * 16), "alloc sorted queries");
   if (partitioned(pr)) {
     RTNN_CU(ensure(ws.qwidth, Q * 4), "alloc widths");
-    RTNN_CU(ensure(ws.fbpos, Q * 4), "alloc fallback list");
-    RTNN_CU(ensure(ws.fbcloud, Q * 4), "alloc fallback list");
+    for (int i = 0; i < 2; ++i) {
+      RTNN_CU(ensure(ws.fbpos[i], Q * 4), "alloc fallback list");
+      RTNN_CU(ensure(ws.fbcloud[i], Q * 4), "alloc fallback list");
+      RTNN_CU(ensure(ws.fbwidth[i], Q * 4), "alloc fallback list");
+    }
   }
   RTNN_CU(ensure(ws.hist, 256 * rt * 4), "alloc radix histogram");
   RTNN_CU(ensure(ws.scan_state, scan_tiles_for(scan_n) * 8), "alloc scan state");
@@ -282,7 +290,7 @@ uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats) {
   const uint32_t passes = sh.Q ? (sh.key_bits + 7) / 8 : 0;
   uint32_t n = (sh.single ? 1 : 0) + 7 + 3 * passes + 1;   // tables, build, sort, gather
   if (partitioned(pr) || feats) n += 1;                      // widths
-  n += partitioned(pr) ? 2 : 1;                              // search (+ fallback)
+  n += partitioned(pr) ? 2 + fallback_passes_of(pr) : 1;     // search (+ fallback passes)
   return n;
 }
 
@@ -303,7 +311,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
 
   RTNN_CU(launch_bbox(d_pts, sh.N, ap, t, sh.n_chunks, (uint32_t*)ws.bbox.p, s), "bbox");
   RTNN_CU(launch_grid_plan(t, (const uint32_t*)ws.bbox.p, pr.radius, tu.cell_ratio,
-                           sh.cell_budget, sh.morton_bits, sh.cell_capacity, grids, ctr, s),
+                           tu.min_cell_ratio, tu.points_per_cell, sh.cell_budget, sh.morton_bits, sh.cell_capacity, grids, ctr, s),
           "grid plan");
   RTNN_CU(launch_zero_cells(cells, ctr, c->n_sms, s), "zero cells");
   RTNN_CU(launch_count(d_pts, sh.N, ap, t, sh.n_chunks, grids, cells, (uint32_t*)ws.rank.p, ctr, s),
@@ -360,34 +368,37 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.spts = (const float4*)ws.spts.p;
   a.sq = (const float4*)ws.sq.p;
   a.qwidth = part ? (const float*)ws.qwidth.p : nullptr;
-  a.fb_pos = (const uint32_t*)ws.fbpos.p;
-  a.fb_cloud = (const uint32_t*)ws.fbcloud.p;
-  a.fb_out_pos = (uint32_t*)ws.fbpos.p;
-  a.fb_out_cloud = (uint32_t*)ws.fbcloud.p;
   a.out = d_out;
   a.ctr = ctr;
-  a.work = &ctr->work[0];
   a.n_tiles = sh.n_tiles;
   a.radius = pr.radius;
   a.r2 = pr.radius * pr.radius;
   a.k = pr.k;
   a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
             ((pr.flags & RTNN_FLAG_LOCAL_INDICES) ? kSearchLocalIndices : 0u);
-  a.fallback_pass = false;
   const int wpb = (int)std::max(1u, std::min(8u, tu.warps_per_block));
   int bps = search_blocks_per_sm(knn, pr.k, wpb);
   if (tu.blocks_per_sm > 0) bps = std::min(bps, (int)tu.blocks_per_sm);
   const uint64_t persistent = (uint64_t)c->n_sms * bps;
   const uint64_t need_blocks = (sh.n_tiles + wpb - 1) / wpb;
-  const unsigned blocks1 = (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
-  RTNN_CU(launch_search(knn, a, blocks1, wpb, s), "search");
-  if (part) {
-    a.fallback_pass = true;
-    a.work = &ctr->work[1];
-    a.qwidth = nullptr;
-    RTNN_CU(launch_search(knn, a, (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks)),
-                          wpb, s),
-            "fallback search");
+  const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
+  // pass 0: every query at its partition width; short queries go to list 0 at twice the
+  // width; escalation pass p reads list (p-1)%2 and writes list p%2; the final pass
+  // searches what is left at the full radius.
+  const int n_fb = part ? (int)fallback_passes_of(pr) : 0;
+  for (int p = 0; p <= (part ? n_fb + 1 : 0); ++p) {
+    a.pass = p == 0 ? kPassMain : (p <= n_fb ? kPassEscalate : kPassFinal);
+    a.work = &ctr->work[p];
+    const int in = (p + 1) & 1, outl = p & 1;
+    a.fb_in_pos = (const uint32_t*)ws.fbpos[in].p;
+    a.fb_in_cloud = (const uint32_t*)ws.fbcloud[in].p;
+    a.fb_in_width = (const float*)ws.fbwidth[in].p;
+    a.fb_in_count = p > 0 ? &ctr->fb_count[p - 1] : nullptr;
+    a.fb_out_pos = (uint32_t*)ws.fbpos[outl].p;
+    a.fb_out_cloud = (uint32_t*)ws.fbcloud[outl].p;
+    a.fb_out_width = (float*)ws.fbwidth[outl].p;
+    a.fb_out_count = &ctr->fb_count[p];
+    RTNN_CU(launch_search(knn, a, blocks, wpb, s), p == 0 ? "search" : "fallback search");
   }
   if (ev) RTNN_CU(cudaEventRecord(ev[3], s), "event");
   return RTNN_OK;
@@ -414,7 +425,7 @@ rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& 
     stats->n_queries = sh.Q;
     stats->n_clouds = sh.n_clouds;
     stats->n_buckets = partitioned(pr) ? 2 : 1;
-    stats->n_fallback = h.fb_count;
+    stats->n_fallback = partitioned(pr) ? h.fb_count[0] : 0;
     stats->n_tiles = sh.n_tiles;
     stats->n_cells = h.total_cells;
     stats->cell_size = c->h_grid->cell;
@@ -552,6 +563,8 @@ rtnn_status rtnn_get_tuning(const rtnn_ctx* c, rtnn_tuning* t) {
 rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
   if (!c || !t) return RTNN_ERR_INVALID_ARGUMENT;
   if (!(t->cell_ratio > 0.f && t->cell_ratio <= 64.f) || !(t->cell_budget > 0.f) ||
+      !(t->min_cell_ratio > 0.f && t->min_cell_ratio <= t->cell_ratio) ||
+      !(t->points_per_cell >= 0.f) || t->fallback_passes > kMaxPasses - 2 ||
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
@@ -573,7 +586,7 @@ rtnn_status rtnn_search(rtnn_ctx* c, const float* points, uint64_t n_points, con
   if (flags & RTNN_FLAG_LOCAL_INDICES) flags &= ~RTNN_FLAG_LOCAL_INDICES;  // one cloud: same
   cudaSetDevice(c->device);
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
-  const Params pr{mode, radius, k, flags};
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
   return run_search(c, sh, pr, points, queries, out, stats);
 }
 
@@ -595,7 +608,7 @@ rtnn_status rtnn_search_batched(rtnn_ctx* c, const float* points, const uint64_t
   if (sh.N > 0 && !points) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "points is NULL");
   if (sh.Q > 0 && !out) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "out is NULL");
   cudaSetDevice(c->device);
-  const Params pr{mode, radius, k, flags};
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
   st = reserve(c, c->ws, sh, pr);
   if (st != RTNN_OK) return st;
   cudaStream_t s = stream_of(c);
@@ -621,7 +634,7 @@ rtnn_status rtnn_plan_create(rtnn_ctx* c, rtnn_plan** plan, const uint64_t* poin
   if (st == RTNN_OK && (p->sh.N == 0 || p->sh.Q == 0))
     st = fail(c, RTNN_ERR_INVALID_ARGUMENT, "a plan needs at least one point and one query");
   if (st != RTNN_OK) { delete p; return st; }
-  p->pr = Params{mode, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS};
+  p->pr = Params{mode, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS, c->tuning.fallback_passes};
   p->use_graph = use_graph != 0;
   cudaSetDevice(c->device);
   st = reserve(c, p->ws, p->sh, p->pr);
@@ -729,7 +742,7 @@ rtnn_status rtnn_collect_training(rtnn_ctx* c, const float* d_points, uint64_t n
   RTNN_CU(ensure(c->ws.cellsz, n_queries * 4), "alloc cell sizes");
   RTNN_CU(ensure(c->ws.kth, n_queries * 4), "alloc kth");
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
-  const Params pr{mode, radius, k, flags};
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
   int32_t* rows = (int32_t*)c->ws.out.p;
   st = run_search(c, sh, pr, d_points, d_queries, rows, nullptr, d_feats, (float*)c->ws.cellsz.p);
   if (st != RTNN_OK) return st;

@@ -119,8 +119,9 @@ k_bbox(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cloud
 // its budget of max(64, cell_budget * points) cells.
 __global__ void __launch_bounds__(1024)
 k_grid_plan(CloudTables t, const uint32_t* __restrict__ bbox, float radius, float cell_ratio,
-            float cell_budget, uint32_t morton_bits, uint64_t cell_capacity,
-            CloudGrid* __restrict__ grids, Counters* ctr) {
+            float min_cell_ratio, float points_per_cell, float cell_budget,
+            uint32_t morton_bits, uint64_t cell_capacity, CloudGrid* __restrict__ grids,
+            Counters* ctr) {
   __shared__ uint32_t s_sum[32];
   __shared__ uint64_t s_carry;
   if (threadIdx.x == 0) s_carry = 0;
@@ -143,6 +144,14 @@ k_grid_plan(CloudTables t, const uint32_t* __restrict__ bbox, float radius, floa
       }
       const double budget = fmin(fmax(64.0, (double)cell_budget * (double)np), 2147483647.0);
       float cell = radius * cell_ratio;
+      if (points_per_cell > 0.f && np > 0) {
+        // dense cloud: shrink the cell until its box holds ~points_per_cell per cell
+        const float lo = radius * min_cell_ratio;
+        double vol = 1.0;
+        for (int a = 0; a < 3; ++a) vol *= fmax((double)(mx[a] - mn[a]), (double)lo);
+        const float cd = (float)cbrt(vol * (double)points_per_cell / (double)np);
+        cell = fminf(cell, fmaxf(cd, lo));
+      }
       int d[3] = {1, 1, 1};
       bool fits = false;
       for (int it = 0; it < 64 && !fits; ++it) {
@@ -323,11 +332,11 @@ cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const
 }
 
 cudaError_t launch_grid_plan(const CloudTables& t, const uint32_t* bbox, float radius,
-                             float cell_ratio, float cell_budget, uint32_t morton_bits,
-                             uint64_t cell_capacity, CloudGrid* grids, Counters* ctr,
-                             cudaStream_t s) {
-  k_grid_plan<<<1, 1024, 0, s>>>(t, bbox, radius, cell_ratio, cell_budget, morton_bits,
-                                 cell_capacity, grids, ctr);
+                             float cell_ratio, float min_cell_ratio, float points_per_cell,
+                             float cell_budget, uint32_t morton_bits, uint64_t cell_capacity,
+                             CloudGrid* grids, Counters* ctr, cudaStream_t s) {
+  k_grid_plan<<<1, 1024, 0, s>>>(t, bbox, radius, cell_ratio, min_cell_ratio, points_per_cell,
+                                 cell_budget, morton_bits, cell_capacity, grids, ctr);
   return cudaGetLastError();
 }
 

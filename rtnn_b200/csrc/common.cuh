@@ -23,6 +23,7 @@ constexpr int kRadixThreads = 256;  // 8 warps
 constexpr int kRadixItems = 16;     // per lane, per warp sub-tile of 512
 constexpr int kRadixTile = kRadixThreads * kRadixItems; // 4096 keys per block
 constexpr int kMaxK = 128;
+constexpr int kMaxPasses = 8;       // main search pass + escalating fallback passes
 
 // Device error codes (first one wins, written with atomicCAS into Counters::error).
 enum DevError : uint32_t {
@@ -48,12 +49,11 @@ struct __align__(16) CloudGrid {
 struct Counters {
   uint32_t error;          // DevError
   uint32_t error_info;     // extra detail (e.g. scan tile that timed out)
-  uint32_t work[4];        // persistent-kernel work queues
-  uint32_t fb_count;       // queries appended to the fallback list
+  uint32_t work[kMaxPasses];      // persistent-kernel work queue of each search pass
+  uint32_t fb_count[kMaxPasses];  // queries appended to the fallback list by each pass
   uint32_t total_cells;    // sum of cloud cells (written by k_grid_plan)
   uint32_t scan_tiles[16]; // dynamic tile counters, one per scan invocation
-  uint64_t n_hits;         // optional statistics
-  uint32_t pad[6];
+  uint32_t pad[3];
 };
 
 // Tables describing the clouds of one pipeline (all device arrays of n_clouds + 1).

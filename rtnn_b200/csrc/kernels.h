@@ -17,20 +17,30 @@ struct SearchArgs {
   const float4* spts;          // cell-sorted points {x, y, z, index}
   const float4* sq;            // Morton-sorted queries {x, y, z, query index}
   const float* qwidth;         // per sorted query search width; nullptr: full radius
-  const uint32_t* fb_pos;      // fallback pass: sorted positions to re-search
-  const uint32_t* fb_cloud;    //                and their clouds
-  uint32_t* fb_out_pos;        // first pass: where narrowed-but-short queries go
+  // fallback passes read the list the previous pass wrote (sorted position, cloud,
+  // width to search at) ...
+  const uint32_t* fb_in_pos;
+  const uint32_t* fb_in_cloud;
+  const float* fb_in_width;
+  const uint32_t* fb_in_count;
+  // ... and append the queries that are still short, with the width doubled
+  uint32_t* fb_out_pos;
   uint32_t* fb_out_cloud;
+  float* fb_out_width;
+  uint32_t* fb_out_count;
   int32_t* out;                // [Q][k]
   Counters* ctr;
   uint32_t* work;              // work-queue counter of this pass
-  uint32_t n_tiles;            // first pass tile count
+  uint32_t n_tiles;            // main pass tile count
   float radius;                // user radius r
   float r2;                    // fl(r * r)
   uint32_t k;
   uint32_t flags;              // kSearch*
-  bool fallback_pass;
+  int pass;                    // kPassMain, kPassEscalate or kPassFinal
 };
+constexpr int kPassMain = 0;      // sorted queries, widths from the partition
+constexpr int kPassEscalate = 1;  // fallback list at its (doubled) widths
+constexpr int kPassFinal = 2;     // fallback list at the full radius (always complete)
 
 // scan.cu
 uint64_t scan_tiles_for(uint64_t n);
@@ -51,9 +61,9 @@ cudaError_t launch_single_tables(uint32_t* tab, uint32_t n_points, uint32_t n_qu
 cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
                         uint32_t n_chunks, uint32_t* bbox, cudaStream_t s);
 cudaError_t launch_grid_plan(const CloudTables& t, const uint32_t* bbox, float radius,
-                             float cell_ratio, float cell_budget, uint32_t morton_bits,
-                             uint64_t cell_capacity, CloudGrid* grids, Counters* ctr,
-                             cudaStream_t s);
+                             float cell_ratio, float min_cell_ratio, float points_per_cell,
+                             float cell_budget, uint32_t morton_bits, uint64_t cell_capacity,
+                             CloudGrid* grids, Counters* ctr, cudaStream_t s);
 cudaError_t launch_zero_cells(uint32_t* cells, const Counters* ctr, int n_sms, cudaStream_t s);
 cudaError_t launch_count(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
                          uint32_t n_chunks, const CloudGrid* grids, uint32_t* cells,

@@ -66,8 +66,9 @@ k_search(SearchArgs a) {
   const uint32_t k = a.k;
   const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
   const bool local_idx = (a.flags & kSearchLocalIndices) != 0;
-  const uint32_t fb_total = a.fallback_pass ? a.ctr->fb_count : 0u;
-  const uint32_t n_tiles = a.fallback_pass ? (fb_total + 31) / 32 : a.n_tiles;
+  const bool main_pass = a.pass == kPassMain;
+  const uint32_t fb_total = main_pass ? 0u : *a.fb_in_count;
+  const uint32_t n_tiles = main_pass ? a.n_tiles : (fb_total + 31) / 32;
   const uint32_t total_cells = a.ctr->total_cells;
 
   while (true) {
@@ -78,25 +79,25 @@ k_search(SearchArgs a) {
 
     bool valid;
     uint32_t pos, cloud;
-    if (!a.fallback_pass) {
+    float wq = a.radius;
+    if (main_pass) {
       uint32_t c = 0;
       if (lane == 0) c = find_cloud(a.t.tile_base, a.t.n_clouds, tile);
       cloud = __shfl_sync(0xffffffffu, c, 0);
       const uint32_t q0 = a.t.query_off[cloud] + (tile - a.t.tile_base[cloud]) * 32u;
       pos = q0 + lane;
       valid = pos < a.t.query_off[cloud + 1];
+      if (valid && a.qwidth) wq = a.qwidth[pos];
     } else {
       const uint32_t e = tile * 32u + lane;
       valid = e < fb_total;
-      pos = valid ? a.fb_pos[e] : 0u;
-      cloud = valid ? a.fb_cloud[e] : 0u;
+      pos = valid ? a.fb_in_pos[e] : 0u;
+      cloud = valid ? a.fb_in_cloud[e] : 0u;
+      if (valid && a.pass == kPassEscalate) wq = a.fb_in_width[e];
     }
     float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
     float w = a.radius, lim = a.r2;
-    if (valid && !a.fallback_pass && a.qwidth) {
-      const float wq = a.qwidth[pos];
-      if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
-    }
+    if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
     valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
 
     uint32_t pending = __ballot_sync(0xffffffffu, valid);
@@ -202,12 +203,13 @@ k_search(SearchArgs a) {
       const uint32_t fbm = __ballot_sync(0xffffffffu, incomplete);
       if (fbm) {
         uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&a.ctr->fb_count, (uint32_t)__popc(fbm));
+        if (lane == 0) base = atomicAdd(a.fb_out_count, (uint32_t)__popc(fbm));
         base = __shfl_sync(0xffffffffu, base, 0);
         if (incomplete) {
           const uint32_t e = base + __popc(fbm & lt);
           a.fb_out_pos[e] = pos;
           a.fb_out_cloud[e] = gcloud;
+          a.fb_out_width[e] = fminf(2.f * w, a.radius);   // next pass: twice as wide
         }
       }
       if (done && sorted_rows) {
