@@ -49,6 +49,13 @@ rtnn_status rtnn_model_train(rtnn_ctx* ctx, const float* d_feats, const float* d
                              uint64_t n, uint32_t epochs, uint32_t batch, float lr,
                              uint64_t seed, float* loss_per_epoch);
 
+/* The search width of every query under the partition (analytic, or the loaded model
+ * with RTNN_FLAG_LEARNED), in query order; d_widths[q] >= radius means the full radius.
+ * Runs the whole partitioned search of one cloud (rows discarded). */
+rtnn_status rtnn_query_widths(rtnn_ctx* ctx, const float* d_points, uint64_t n_points,
+                              const float* d_queries, uint64_t n_queries, rtnn_mode mode,
+                              float radius, uint32_t k, uint32_t flags, float* d_widths);
+
 /* Building blocks, exposed for gradient checks. d_grad receives the SUM over the batch
  * of d(0.5 * (o - t_n)^2)/d(theta) for the trained parameters; d_loss the summed loss.
  * o is the normalised network output, t_n = (target - out_mean) / out_std. */

@@ -101,6 +101,7 @@ _SIGS = {
     "rtnn_model_get": (_I, [_P, _P, _U32]),
     "rtnn_collect_training": (_I, [_P, _P, _U64, _P, _U64, _I, _F, _U32, _P, _P]),
     "rtnn_model_train": (_I, [_P, _P, _P, _U64, _U32, _U32, _F, _U64, _P]),
+    "rtnn_query_widths": (_I, [_P, _P, _U64, _P, _U64, _I, _F, _U32, _U32, _P]),
     "rtnn_mlp_loss_grad": (_I, [_P, _P, _P, _P, _U32, _P, _P]),
     "rtnn_mlp_forward": (_I, [_P, _P, _P, _U32, _P]),
     "rtnn_mlp_adam_step": (_I, [_P, _P, _P, _P, _P, _F, _U32, _F]),
@@ -299,6 +300,17 @@ class Context:
             self._h, _P(feats.data_ptr()), _P(target.data_ptr()), feats.shape[0], int(epochs),
             int(batch), float(lr), int(seed), losses.ctypes.data_as(_P)))
         return losses
+
+    def query_widths(self, points, queries=None, mode="knn", radius=2.0, k=16, learned=False):
+        """Per-query partition widths (CUDA tensor, query order)."""
+        import torch
+        nq = points.shape[0] if queries is None else queries.shape[0]
+        w = torch.empty((nq,), dtype=torch.float32, device=points.device)
+        self._check(load_library().rtnn_query_widths(
+            self._h, _P(points.data_ptr()), points.shape[0],
+            _P(queries.data_ptr()) if queries is not None else None, nq, _mode(mode),
+            float(radius), int(k), FLAG_LEARNED if learned else 0, _P(w.data_ptr())))
+        return w
 
     def mlp_loss_grad(self, params, feats, target):
         import torch

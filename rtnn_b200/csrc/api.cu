@@ -55,11 +55,11 @@ void release(DevBuf& b) {
 
 struct Workspace {
   DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth,
-      fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters, in_pts, in_qs, out, feats,
+      qwidth_in, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters, in_pts, in_qs, out, feats,
       cellsz, kth;
   void release_all() {
     for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
-                      &vals1, &sq, &qwidth, &fbpos[0], &fbpos[1], &fbcloud[0], &fbcloud[1],
+                      &vals1, &sq, &qwidth, &qwidth_in, &fbpos[0], &fbpos[1], &fbcloud[0], &fbcloud[1],
                       &fbwidth[0], &fbwidth[1], &hist, &scan_state, &counters,
                       &in_pts, &in_qs, &out, &feats, &cellsz, &kth})
       release(*b);
@@ -162,7 +162,7 @@ void finish_shapes(Shapes& sh, const rtnn_tuning& tu) {
   uint32_t mb = (ceil_log2(std::max<uint64_t>(sh.max_cloud_q, 2)) + 2) / 3;
   mb = std::max(1u, std::min(10u, mb));
   const uint32_t cb = ceil_log2(sh.n_clouds);
-  if (cb + 3 * mb > 64) mb = (64 - cb) / 3;
+  if (cb + 3 * mb + 4 > 64) mb = (60 - cb) / 3;   // room for 4 density-bucket bits
   sh.morton_bits = mb;
   sh.key_bits = std::max(8u, cb + 3 * mb);
   sh.key64 = sh.key_bits > 32;
@@ -238,6 +238,9 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
 }
 
 bool partitioned(const Params& p) { return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0; }
+uint32_t level_bits_of(const Params& p) { return partitioned(p) ? 4u : 0u; }
+uint32_t key_bits_of(const Shapes& sh, const Params& p) { return sh.key_bits + level_bits_of(p); }
+bool key64_of(const Shapes& sh, const Params& p) { return key_bits_of(sh, p) > 32; }
 
 uint32_t fallback_passes_of(const Params& p) { return p.fb_passes; }
 
@@ -252,13 +255,14 @@ rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& 
   RTNN_CU(ensure(ws.cells, (sh.cell_capacity + 1) * 4), "alloc cells");
   RTNN_CU(ensure(ws.rank, N * 4), "alloc rank");
   RTNN_CU(ensure(ws.spts, N * 16), "alloc sorted points");
-  RTNN_CU(ensure(ws.keys0, Q * (sh.key64 ? 8 : 4)), "alloc keys");
-  RTNN_CU(ensure(ws.keys1, Q * (sh.key64 ? 8 : 4)), "alloc keys");
+  RTNN_CU(ensure(ws.keys0, Q * (key64_of(sh, pr) ? 8 : 4)), "alloc keys");
+  RTNN_CU(ensure(ws.keys1, Q * (key64_of(sh, pr) ? 8 : 4)), "alloc keys");
   RTNN_CU(ensure(ws.vals0, Q * 4), "alloc vals");
   RTNN_CU(ensure(ws.vals1, Q * 4), "alloc vals");
   RTNN_CU(ensure(ws.sq, Q * 16), "alloc sorted queries");
   if (partitioned(pr)) {
     RTNN_CU(ensure(ws.qwidth, Q * 4), "alloc widths");
+    RTNN_CU(ensure(ws.qwidth_in, Q * 4), "alloc widths");
     for (int i = 0; i < 2; ++i) {
       RTNN_CU(ensure(ws.fbpos[i], Q * 4), "alloc fallback list");
       RTNN_CU(ensure(ws.fbcloud[i], Q * 4), "alloc fallback list");
@@ -287,7 +291,7 @@ CloudTables tables_of(const Workspace& ws, uint32_t n_clouds) {
 // Issues the whole pipeline on stream s. ev: 4 events (or nullptr) bracketing
 // build | partition | search.
 uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats) {
-  const uint32_t passes = sh.Q ? (sh.key_bits + 7) / 8 : 0;
+  const uint32_t passes = sh.Q ? (key_bits_of(sh, pr) + 7) / 8 : 0;
   uint32_t n = (sh.single ? 1 : 0) + 7 + 3 * passes + 1;   // tables, build, sort, gather
   if (partitioned(pr) || feats) n += 1;                      // widths
   n += partitioned(pr) ? 2 + fallback_passes_of(pr) : 1;     // search (+ fallback passes)
@@ -322,27 +326,17 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   RTNN_CU(launch_scatter(d_pts, sh.N, ap, t, sh.n_chunks, grids, cells, (uint32_t*)ws.rank.p,
                          (float4*)ws.spts.p, ctr, s),
           "scatter");
-  RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.morton_bits, sh.key64,
-                            ws.keys0.p, nullptr, s),
-          "query keys");
-  bool in1 = false;
-  RTNN_CU(radix_sort_pairs(sh.key64, ws.keys0.p, (uint32_t*)ws.vals0.p, ws.keys1.p,
-                           (uint32_t*)ws.vals1.p, (uint32_t)sh.Q, sh.key_bits, true,
-                           (uint32_t*)ws.hist.p, (uint64_t*)ws.scan_state.p, &ctr->scan_tiles[1],
-                           ctr, &in1, s),
-          "radix sort");
-  const uint32_t* order = (const uint32_t*)(in1 ? ws.vals1.p : ws.vals0.p);
-  RTNN_CU(launch_gather_queries(d_qs, order, (uint32_t)sh.Q, (float4*)ws.sq.p, c->n_sms, s),
-          "gather queries");
   if (ev) RTNN_CU(cudaEventRecord(ev[1], s), "event");
 
+  // density buckets: a width per query (caller's order), then the sort key
+  // cloud | bucket of the width | Morton code, so each 32-query tile shares one width
   const bool part = partitioned(pr);
   if (part || feats_out) {
     WidthArgs w{};
     w.t = t;
     w.grids = grids;
     w.cells = cells;
-    w.sq = (const float4*)ws.sq.p;
+    w.xyz = d_qs;
     w.total_cells = &ctr->total_cells;
     w.n_queries = (uint32_t)sh.Q;
     w.radius = pr.radius;
@@ -350,15 +344,27 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     w.alpha = 1.24f;   // equal-volume radius of a (2s+2)-cell cube, util.cpp:422-426
     w.model = (pr.flags & RTNN_FLAG_LEARNED) ? (const float*)c->model.p : nullptr;
     w.margin = tu.width_margin;
-    w.qwidth = part ? (float*)ws.qwidth.p : nullptr;
+    w.qwidth = (float*)ws.qwidth_in.p;
     w.feats = feats_out;
     w.cellsz = cellsz_out;
-    if (!part) {   // features only: widths land in a scratch buffer
-      RTNN_CU(ensure(ws.qwidth, std::max<uint64_t>(sh.Q, 1) * 4), "alloc widths");
-      w.qwidth = (float*)ws.qwidth.p;
-    }
     RTNN_CU(launch_widths(w, c->n_sms, s), "widths");
   }
+  const bool key64 = key64_of(sh, pr);
+  RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.morton_bits,
+                            part ? (const float*)ws.qwidth_in.p : nullptr, pr.radius,
+                            level_bits_of(pr), key64, ws.keys0.p, s),
+          "query keys");
+  bool in1 = false;
+  RTNN_CU(radix_sort_pairs(key64, ws.keys0.p, (uint32_t*)ws.vals0.p, ws.keys1.p,
+                           (uint32_t*)ws.vals1.p, (uint32_t)sh.Q, key_bits_of(sh, pr), true,
+                           (uint32_t*)ws.hist.p, (uint64_t*)ws.scan_state.p, &ctr->scan_tiles[1],
+                           ctr, &in1, s),
+          "radix sort");
+  const uint32_t* order = (const uint32_t*)(in1 ? ws.vals1.p : ws.vals0.p);
+  RTNN_CU(launch_gather_queries(d_qs, order, (uint32_t)sh.Q, (float4*)ws.sq.p,
+                                part ? (const float*)ws.qwidth_in.p : nullptr,
+                                part ? (float*)ws.qwidth.p : nullptr, c->n_sms, s),
+          "gather queries");
   if (ev) RTNN_CU(cudaEventRecord(ev[2], s), "event");
 
   SearchArgs a{};
@@ -741,6 +747,7 @@ rtnn_status rtnn_collect_training(rtnn_ctx* c, const float* d_points, uint64_t n
   RTNN_CU(ensure(c->ws.out, (size_t)n_queries * k * 4), "alloc rows");
   RTNN_CU(ensure(c->ws.cellsz, n_queries * 4), "alloc cell sizes");
   RTNN_CU(ensure(c->ws.kth, n_queries * 4), "alloc kth");
+  RTNN_CU(ensure(c->ws.qwidth_in, n_queries * 4), "alloc widths");
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
   const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
   int32_t* rows = (int32_t*)c->ws.out.p;
@@ -759,6 +766,29 @@ rtnn_status rtnn_collect_training(rtnn_ctx* c, const float* d_points, uint64_t n
     tgt[i] = std::log(d / cz[i]);
   }
   RTNN_CU(cudaMemcpyAsync(d_target, tgt.data(), n_queries * 4, cudaMemcpyHostToDevice, s), "copy");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_query_widths(rtnn_ctx* c, const float* d_points, uint64_t n_points,
+                              const float* d_queries, uint64_t n_queries, rtnn_mode mode,
+                              float radius, uint32_t k, uint32_t flags, float* d_widths) {
+  if (!c || !d_points || !d_widths) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  if (d_queries == nullptr) n_queries = n_points;
+  flags = (flags & RTNN_FLAG_LEARNED) | RTNN_FLAG_PARTITION | RTNN_FLAG_DEVICE_POINTERS;
+  rtnn_status st = check_args(c, n_points, n_queries, radius, k, flags);
+  if (st != RTNN_OK) return st;
+  if (n_points == 0 || n_queries == 0) return RTNN_OK;
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  RTNN_CU(ensure(c->ws.out, (size_t)n_queries * k * 4), "alloc rows");
+  const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
+  st = run_search(c, sh, pr, d_points, d_queries, (int32_t*)c->ws.out.p, nullptr);
+  if (st != RTNN_OK) return st;
+  RTNN_CU(cudaMemcpyAsync(d_widths, c->ws.qwidth_in.p, n_queries * 4, cudaMemcpyDeviceToDevice, s),
+          "copy widths");
   RTNN_CU(cudaStreamSynchronize(s), "synchronize");
   return RTNN_OK;
 }
@@ -818,7 +848,7 @@ rtnn_status rtnn_model_train(rtnn_ctx* c, const float* d_feats, const float* d_t
     for (uint64_t i = 0; i < n; ++i) { const double d = f[i * kFeatDim + j] - m; v += d * d; }
     v /= (double)n;
     P[j] = (float)m;
-    P[kFeatDim + j] = (float)std::max(std::sqrt(v), 1e-3);
+    P[kFeatDim + j] = (float)(std::sqrt(v) < 1e-2 ? 1.0 : std::sqrt(v));   // constant feature: identity scale
   }
   {
     double m = 0, v = 0;

@@ -272,12 +272,21 @@ k_scatter(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cl
   }
 }
 
-// Morton key per query: (cloud << 3*mbits) | morton(cell coords >> shift).
+// Density bucket of a width: 0 for the full radius, then two buckets per halving.
+__device__ __forceinline__ uint32_t width_level(float w, float radius, uint32_t level_bits) {
+  if (!(w < radius)) return 0u;
+  const uint32_t top = (1u << level_bits) - 1u;
+  const float l = ceilf(-2.f * log2f(fmaxf(w, 1e-30f) / radius));
+  return (uint32_t)fminf(fmaxf(l, 1.f), (float)top);
+}
+
+// Sort key per query: cloud | density bucket of its width | Morton code of its cell.
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
 k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
              CloudTables t, const CloudGrid* __restrict__ grids, uint32_t morton_bits,
-             KeyT* __restrict__ keys, uint32_t* __restrict__ vals) {
+             const float* __restrict__ qwidth, float radius, uint32_t level_bits,
+             KeyT* __restrict__ keys) {
   __shared__ float s_xyz[kChunk * 3];
   const ChunkRange r = chunk_range(t.qchunk_base, t.query_off, t.n_clouds, blockIdx.x);
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
@@ -288,18 +297,21 @@ k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
     const int cz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.inv_cell), g.dz);
     const uint32_t m = morton3((uint32_t)cx >> g.morton_shift, (uint32_t)cy >> g.morton_shift,
                                (uint32_t)cz >> g.morton_shift);
-    keys[r.begin + i] = ((KeyT)r.cloud << (3 * morton_bits)) | (KeyT)m;
-    if (vals) vals[r.begin + i] = r.begin + i;
+    const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits) : 0u;
+    keys[r.begin + i] = ((KeyT)r.cloud << (3 * morton_bits + level_bits)) |
+                        ((KeyT)lvl << (3 * morton_bits)) | (KeyT)m;
   }
 }
 
-// Sorted queries as float4 {x, y, z, original query index}.
+// Sorted queries as float4 {x, y, z, original query index} (+ their widths).
 __global__ void k_gather_queries(const float* __restrict__ xyz, const uint32_t* __restrict__ order,
-                                 uint32_t n, float4* __restrict__ sq) {
+                                 uint32_t n, float4* __restrict__ sq,
+                                 const float* __restrict__ w_in, float* __restrict__ w_out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t q = order[i];
     const float* p = xyz + 3ull * q;
     sq[i] = make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __uint_as_float(q));
+    if (w_in) w_out[i] = __ldg(w_in + q);
   }
 }
 
@@ -365,23 +377,26 @@ cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
 
 cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
                               const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
-                              uint32_t morton_bits, bool key64, void* keys, uint32_t* vals,
-                              cudaStream_t s) {
+                              uint32_t morton_bits, const float* qwidth, float radius,
+                              uint32_t level_bits, bool key64, void* keys, cudaStream_t s) {
   if (n_qchunks == 0) return cudaSuccess;
   if (key64)
     k_query_keys<uint64_t><<<n_qchunks, 256, 0, s>>>(xyz, 3 * n_queries, aligned, t, grids,
-                                                     morton_bits, (uint64_t*)keys, vals);
+                                                     morton_bits, qwidth, radius, level_bits,
+                                                     (uint64_t*)keys);
   else
     k_query_keys<uint32_t><<<n_qchunks, 256, 0, s>>>(xyz, 3 * n_queries, aligned, t, grids,
-                                                     morton_bits, (uint32_t*)keys, vals);
+                                                     morton_bits, qwidth, radius, level_bits,
+                                                     (uint32_t*)keys);
   return cudaGetLastError();
 }
 
 cudaError_t launch_gather_queries(const float* xyz, const uint32_t* order, uint32_t n,
-                                  float4* sq, int n_sms, cudaStream_t s) {
+                                  float4* sq, const float* w_in, float* w_out, int n_sms,
+                                  cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   unsigned blocks = (unsigned)min((uint64_t)n_sms * 16, ((uint64_t)n + 255) / 256);
-  k_gather_queries<<<blocks, 256, 0, s>>>(xyz, order, n, sq);
+  k_gather_queries<<<blocks, 256, 0, s>>>(xyz, order, n, sq, w_in, w_out);
   return cudaGetLastError();
 }
 

@@ -74,10 +74,11 @@ cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
                            Counters* ctr, cudaStream_t s);
 cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
                               const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
-                              uint32_t morton_bits, bool key64, void* keys, uint32_t* vals,
-                              cudaStream_t s);
+                              uint32_t morton_bits, const float* qwidth, float radius,
+                              uint32_t level_bits, bool key64, void* keys, cudaStream_t s);
 cudaError_t launch_gather_queries(const float* xyz, const uint32_t* order, uint32_t n,
-                                  float4* sq, int n_sms, cudaStream_t s);
+                                  float4* sq, const float* w_in, float* w_out, int n_sms,
+                                  cudaStream_t s);
 
 // search.cu
 size_t search_smem_bytes(uint32_t k, int warps_per_block);
@@ -100,7 +101,7 @@ struct WidthArgs {
   CloudTables t;
   const CloudGrid* grids;
   const uint32_t* cells;
-  const float4* sq;
+  const float* xyz;             // queries in the caller's order (AoS float3)
   const uint32_t* total_cells;  // cells in use (device)
   uint32_t n_queries;
   float radius;

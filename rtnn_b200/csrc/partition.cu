@@ -90,24 +90,29 @@ k_widths(WidthArgs a) {
        i += gridDim.x * blockDim.x) {
     const uint32_t cloud = find_cloud(a.t.query_off, a.t.n_clouds, i);
     const CloudGrid g = a.grids[cloud];
-    const float4 q = a.sq[i];
+    const float qx = __ldg(a.xyz + 3ull * i), qy = __ldg(a.xyz + 3ull * i + 1),
+                qz = __ldg(a.xyz + 3ull * i + 2);
     if ((uint64_t)g.cell_base + g.n_cells > (uint64_t)total_cells) {  // overran: full radius
       a.qwidth[i] = a.radius;
       continue;
     }
-    const int cx = clamp_cell(cell_coord_f(q.x, g.ox, g.inv_cell), g.dx);
-    const int cy = clamp_cell(cell_coord_f(q.y, g.oy, g.inv_cell), g.dy);
-    const int cz = clamp_cell(cell_coord_f(q.z, g.oz, g.inv_cell), g.dz);
+    const int cx = clamp_cell(cell_coord_f(qx, g.ox, g.inv_cell), g.dx);
+    const int cy = clamp_cell(cell_coord_f(qy, g.oy, g.inv_cell), g.dy);
+    const int cz = clamp_cell(cell_coord_f(qz, g.oz, g.inv_cell), g.dz);
     uint32_t N[kShells];
 #pragma unroll
     for (int s = 0; s < kShells; ++s) N[s] = box_count(g, a.cells, cx, cy, cz, s);
+    // offset of the query from its cell's centre, in cells (0 .. 0.87)
+    const float ox = (qx - g.ox) * g.inv_cell - ((float)cx + 0.5f);
+    const float oy = (qy - g.oy) * g.inv_cell - ((float)cy + 0.5f);
+    const float oz = (qz - g.oz) * g.inv_cell - ((float)cz + 0.5f);
     float feat[kFeatDim];
     feat[0] = log1pf((float)N[0]);
     feat[1] = log1pf((float)(N[1] - N[0]));
     feat[2] = log1pf((float)(N[2] - N[1]));
-    feat[3] = log1pf((float)N[2]);
+    feat[3] = logf((float)a.need) - log1pf((float)N[2]);
     feat[4] = logf(g.cell / a.radius);
-    feat[5] = logf((float)a.need);
+    feat[5] = fminf(sqrtf(ox * ox + oy * oy + oz * oz), 1.f);
     float w;
     if (a.model) {
       const float o = mlp_forward_norm(mv, feat);
@@ -120,12 +125,11 @@ k_widths(WidthArgs a) {
         if (w == INFINITY && N[s] >= a.need) w = a.alpha * (float)(s + 1) * g.cell;
     }
     a.qwidth[i] = (w < a.radius) ? w : a.radius;
-    const uint32_t qi = __float_as_uint(q.w);
     if (a.feats) {
 #pragma unroll
-      for (int f = 0; f < kFeatDim; ++f) a.feats[(size_t)qi * kFeatDim + f] = feat[f];
+      for (int f = 0; f < kFeatDim; ++f) a.feats[(size_t)i * kFeatDim + f] = feat[f];
     }
-    if (a.cellsz) a.cellsz[qi] = g.cell;
+    if (a.cellsz) a.cellsz[i] = g.cell;
   }
 }
 
