@@ -74,12 +74,12 @@ typedef struct rtnn_stats {
   uint64_t n_cells;          /* total grid cells over all clouds */
   float cell_size;           /* cell edge of the first cloud */
   uint32_t grid_dims[3];     /* grid dimensions of the first cloud */
-  float ms_build;            /* bounds + grid build + query ordering */
-  float ms_partition;        /* per-query widths (analytic or learned) */
-  float ms_search;           /* both search passes and the output write */
+  float ms_build;            /* bounds, per-cell counts, scan, scatter (grid build) */
+  float ms_partition;        /* per-query widths and the query sort into buckets */
+  float ms_search;           /* every search pass and the output write */
   float ms_total;            /* device time of the whole call (copies excluded) */
   uint32_t n_launches;       /* kernels of this library launched by the call */
-  uint32_t pad;
+  float ms_fallback;         /* the part of ms_search spent after the first pass */
 } rtnn_stats;
 
 typedef struct rtnn_ctx rtnn_ctx;

@@ -55,7 +55,7 @@ class Stats(ctypes.Structure):
         ("grid_dims", ctypes.c_uint32 * 3),
         ("ms_build", ctypes.c_float), ("ms_partition", ctypes.c_float),
         ("ms_search", ctypes.c_float), ("ms_total", ctypes.c_float),
-        ("n_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+        ("n_launches", ctypes.c_uint32), ("ms_fallback", ctypes.c_float),
     ]
 
     def as_dict(self):

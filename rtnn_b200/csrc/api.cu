@@ -55,11 +55,11 @@ void release(DevBuf& b) {
 
 struct Workspace {
   DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth,
-      qwidth_in, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters, in_pts, in_qs, out, feats,
+      qwidth_in, fbflag, fbnextw, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters, in_pts, in_qs, out, feats,
       cellsz, kth;
   void release_all() {
     for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
-                      &vals1, &sq, &qwidth, &qwidth_in, &fbpos[0], &fbpos[1], &fbcloud[0], &fbcloud[1],
+                      &vals1, &sq, &qwidth, &qwidth_in, &fbflag, &fbnextw, &fbpos[0], &fbpos[1], &fbcloud[0], &fbcloud[1],
                       &fbwidth[0], &fbwidth[1], &hist, &scan_state, &counters,
                       &in_pts, &in_qs, &out, &feats, &cellsz, &kth})
       release(*b);
@@ -248,7 +248,7 @@ rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& 
   const uint64_t n1 = sh.n_clouds + 1ull;
   const uint64_t N = std::max<uint64_t>(sh.N, 1), Q = std::max<uint64_t>(sh.Q, 1);
   const uint64_t rt = radix_tiles_for(Q);
-  const uint64_t scan_n = std::max<uint64_t>(sh.cell_capacity + 1, 256ull * rt);
+  const uint64_t scan_n = std::max<uint64_t>(std::max<uint64_t>(sh.cell_capacity + 1, 256ull * rt), Q + 1);
   RTNN_CU(ensure(ws.tables, 5 * n1 * 4), "alloc tables");
   RTNN_CU(ensure(ws.grids, sh.n_clouds * sizeof(CloudGrid)), "alloc grids");
   RTNN_CU(ensure(ws.bbox, 6ull * sh.n_clouds * 4), "alloc bbox");
@@ -268,6 +268,8 @@ rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& 
       RTNN_CU(ensure(ws.fbcloud[i], Q * 4), "alloc fallback list");
       RTNN_CU(ensure(ws.fbwidth[i], Q * 4), "alloc fallback list");
     }
+    RTNN_CU(ensure(ws.fbflag, (Q + 1) * 4), "alloc fallback flags");
+    RTNN_CU(ensure(ws.fbnextw, Q * 4), "alloc fallback widths");
   }
   RTNN_CU(ensure(ws.hist, 256 * rt * 4), "alloc radix histogram");
   RTNN_CU(ensure(ws.scan_state, scan_tiles_for(scan_n) * 8), "alloc scan state");
@@ -294,7 +296,8 @@ uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats) {
   const uint32_t passes = sh.Q ? (key_bits_of(sh, pr) + 7) / 8 : 0;
   uint32_t n = (sh.single ? 1 : 0) + 7 + 3 * passes + 1;   // tables, build, sort, gather
   if (partitioned(pr) || feats) n += 1;                      // widths
-  n += partitioned(pr) ? 2 + fallback_passes_of(pr) : 1;     // search (+ fallback passes)
+  // search passes; each flagging pass adds a flag scan and a compaction
+  n += partitioned(pr) ? 3 * fallback_passes_of(pr) + 4 : 1;
   return n;
 }
 
@@ -388,11 +391,15 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   const uint64_t persistent = (uint64_t)c->n_sms * bps;
   const uint64_t need_blocks = (sh.n_tiles + wpb - 1) / wpb;
   const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
-  // pass 0: every query at its partition width; short queries go to list 0 at twice the
-  // width; escalation pass p reads list (p-1)%2 and writes list p%2; the final pass
-  // searches what is left at the full radius.
+  // pass 0: every query at its partition width; each pass flags its short queries, an
+  // order-preserving compaction (scan of the flags) turns them into list p%2 at twice
+  // the width, and escalation pass p reads list (p-1)%2; the final pass searches what
+  // is left at the full radius. Lists stay in (cloud, bucket, Morton) order, so fallback
+  // tiles remain spatially coherent.
   const int n_fb = part ? (int)fallback_passes_of(pr) : 0;
+  uint32_t* flags = (uint32_t*)ws.fbflag.p;
   for (int p = 0; p <= (part ? n_fb + 1 : 0); ++p) {
+    if (p == 1 && ev) RTNN_CU(cudaEventRecord(ev[3], s), "event");
     a.pass = p == 0 ? kPassMain : (p <= n_fb ? kPassEscalate : kPassFinal);
     a.work = &ctr->work[p];
     const int in = (p + 1) & 1, outl = p & 1;
@@ -400,13 +407,28 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     a.fb_in_cloud = (const uint32_t*)ws.fbcloud[in].p;
     a.fb_in_width = (const float*)ws.fbwidth[in].p;
     a.fb_in_count = p > 0 ? &ctr->fb_count[p - 1] : nullptr;
-    a.fb_out_pos = (uint32_t*)ws.fbpos[outl].p;
-    a.fb_out_cloud = (uint32_t*)ws.fbcloud[outl].p;
-    a.fb_out_width = (float*)ws.fbwidth[outl].p;
-    a.fb_out_count = &ctr->fb_count[p];
+    const bool flagging = part && a.pass != kPassFinal;
+    a.fb_flag = flagging ? flags : nullptr;
+    a.fb_next_w = flagging ? (float*)ws.fbnextw.p : nullptr;
+    if (flagging) RTNN_CU(cudaMemsetAsync(flags, 0, (sh.Q + 1) * 4, s), "memset flags");
     RTNN_CU(launch_search(knn, a, blocks, wpb, s), p == 0 ? "search" : "fallback search");
+    if (flagging) {
+      const uint32_t* n_dev = p > 0 ? &ctr->fb_count[p - 1] : nullptr;
+      RTNN_CU(launch_scan_excl(flags, sh.Q + 1, n_dev, 1, sh.Q + 1, (uint64_t*)ws.scan_state.p,
+                               &ctr->scan_tiles[12 + p], ctr, s),
+              "scan flags");
+      RTNN_CU(launch_compact_fallback(flags, (uint32_t)sh.Q, n_dev, t,
+                                      p > 0 ? a.fb_in_pos : nullptr, p > 0 ? a.fb_in_cloud : nullptr,
+                                      (const float*)ws.fbnextw.p, (uint32_t*)ws.fbpos[outl].p,
+                                      (uint32_t*)ws.fbcloud[outl].p, (float*)ws.fbwidth[outl].p,
+                                      &ctr->fb_count[p], c->n_sms, s),
+              "compact fallback");
+    }
   }
-  if (ev) RTNN_CU(cudaEventRecord(ev[3], s), "event");
+  if (ev) {
+    if (!part) RTNN_CU(cudaEventRecord(ev[3], s), "event");
+    RTNN_CU(cudaEventRecord(ev[4], s), "event");
+  }
   return RTNN_OK;
 }
 
@@ -442,8 +464,9 @@ rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& 
     if (timed) {
       cudaEventElapsedTime(&stats->ms_build, c->ev[0], c->ev[1]);
       cudaEventElapsedTime(&stats->ms_partition, c->ev[1], c->ev[2]);
-      cudaEventElapsedTime(&stats->ms_search, c->ev[2], c->ev[3]);
-      cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[3]);
+      cudaEventElapsedTime(&stats->ms_search, c->ev[2], c->ev[4]);
+      cudaEventElapsedTime(&stats->ms_fallback, c->ev[3], c->ev[4]);
+      cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[4]);
     }
   }
   return RTNN_OK;
@@ -690,9 +713,9 @@ rtnn_status rtnn_plan_execute(rtnn_plan* p, const float* d_points, const float* 
   }
   RTNN_CU(cudaEventRecord(c->ev[0], s), "event");
   RTNN_CU(cudaGraphLaunch(p->exec, s), "graph launch");
-  RTNN_CU(cudaEventRecord(c->ev[3], s), "event");
+  RTNN_CU(cudaEventRecord(c->ev[4], s), "event");
   rtnn_status st = read_back(c, p->ws, s, p->sh, p->pr, stats, false);
-  if (st == RTNN_OK && stats) cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[3]);
+  if (st == RTNN_OK && stats) cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[4]);
   return st;
 }
 

@@ -52,7 +52,7 @@ struct Counters {
   uint32_t work[kMaxPasses];      // persistent-kernel work queue of each search pass
   uint32_t fb_count[kMaxPasses];  // queries appended to the fallback list by each pass
   uint32_t total_cells;    // sum of cloud cells (written by k_grid_plan)
-  uint32_t scan_tiles[16]; // dynamic tile counters, one per scan invocation
+  uint32_t scan_tiles[24]; // dynamic tile counters, one per scan invocation
   uint32_t pad[3];
 };
 

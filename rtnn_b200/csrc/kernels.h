@@ -23,11 +23,10 @@ struct SearchArgs {
   const uint32_t* fb_in_cloud;
   const float* fb_in_width;
   const uint32_t* fb_in_count;
-  // ... and append the queries that are still short, with the width doubled
-  uint32_t* fb_out_pos;
-  uint32_t* fb_out_cloud;
-  float* fb_out_width;
-  uint32_t* fb_out_count;
+  // ... and flag each entry that is still short (flag per entry, and the doubled
+  // width it is retried at); nullptr in the final pass
+  uint32_t* fb_flag;
+  float* fb_next_w;
   int32_t* out;                // [Q][k]
   Counters* ctr;
   uint32_t* work;              // work-queue counter of this pass
@@ -86,6 +85,11 @@ cudaError_t search_prepare(int device);
 int search_blocks_per_sm(bool knn, uint32_t k, int warps_per_block);
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
                           cudaStream_t s);
+cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, const uint32_t* n_dev,
+                                    const CloudTables& t, const uint32_t* in_pos,
+                                    const uint32_t* in_cloud, const float* next_w,
+                                    uint32_t* out_pos, uint32_t* out_cloud, float* out_w,
+                                    uint32_t* out_count, int n_sms, cudaStream_t s);
 
 // partition.cu -- density buckets: per-query search widths (analytic or learned MLP)
 constexpr int kShells = 3;                 // box counts N_0..N_2 around a query's cell

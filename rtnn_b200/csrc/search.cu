@@ -78,7 +78,7 @@ k_search(SearchArgs a) {
     if (tile >= n_tiles) break;
 
     bool valid;
-    uint32_t pos, cloud;
+    uint32_t pos, cloud, entry;
     float wq = a.radius;
     if (main_pass) {
       uint32_t c = 0;
@@ -86,20 +86,23 @@ k_search(SearchArgs a) {
       cloud = __shfl_sync(0xffffffffu, c, 0);
       const uint32_t q0 = a.t.query_off[cloud] + (tile - a.t.tile_base[cloud]) * 32u;
       pos = q0 + lane;
+      entry = pos;
       valid = pos < a.t.query_off[cloud + 1];
       if (valid && a.qwidth) wq = a.qwidth[pos];
     } else {
-      const uint32_t e = tile * 32u + lane;
-      valid = e < fb_total;
-      pos = valid ? a.fb_in_pos[e] : 0u;
-      cloud = valid ? a.fb_in_cloud[e] : 0u;
-      if (valid && a.pass == kPassEscalate) wq = a.fb_in_width[e];
+      entry = tile * 32u + lane;
+      valid = entry < fb_total;
+      pos = valid ? a.fb_in_pos[entry] : 0u;
+      cloud = valid ? a.fb_in_cloud[entry] : 0u;
+      if (valid && a.pass == kPassEscalate) wq = a.fb_in_width[entry];
     }
+    const bool in_range = valid;
     float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
     float w = a.radius, lim = a.r2;
     if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
     valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
 
+    bool short_lane = false;   // narrowed search that found fewer than K neighbors
     uint32_t pending = __ballot_sync(0xffffffffu, valid);
     while (pending) {
       const int leader = __ffs(pending) - 1;
@@ -200,18 +203,7 @@ k_search(SearchArgs a) {
       // completion: a narrowed search that found fewer than K neighbors is redone at r
       const bool incomplete = act && (lim_l < a.r2) && (n < k);
       const bool done = act && !incomplete;
-      const uint32_t fbm = __ballot_sync(0xffffffffu, incomplete);
-      if (fbm) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(a.fb_out_count, (uint32_t)__popc(fbm));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (incomplete) {
-          const uint32_t e = base + __popc(fbm & lt);
-          a.fb_out_pos[e] = pos;
-          a.fb_out_cloud[e] = gcloud;
-          a.fb_out_width[e] = fminf(2.f * w, a.radius);   // next pass: twice as wide
-        }
-      }
+      if (act) short_lane = incomplete;
       if (done && sorted_rows) {
         for (uint32_t i = 1; i < n; ++i) {
           const uint64_t x = heap[i * 32];
@@ -238,10 +230,45 @@ k_search(SearchArgs a) {
       }
       __syncwarp();
     }
+    // flag per entry; the compaction keeps the flagged ones in this pass's order
+    if (a.fb_flag && in_range) {
+      a.fb_flag[entry] = short_lane ? 1u : 0u;
+      if (short_lane) a.fb_next_w[entry] = fminf(2.f * w, a.radius);  // twice as wide next
+    }
+  }
+}
+
+// Order-preserving compaction of the short queries of a pass: flags were scanned in
+// place (n + 1 entries, flags[n] = total), entry e is short when flags[e+1] > flags[e].
+__global__ void k_compact_fallback(const uint32_t* __restrict__ flags, uint32_t n_host,
+                                   const uint32_t* n_dev, CloudTables t,
+                                   const uint32_t* __restrict__ in_pos,
+                                   const uint32_t* __restrict__ in_cloud,
+                                   const float* __restrict__ next_w, uint32_t* __restrict__ out_pos,
+                                   uint32_t* __restrict__ out_cloud, float* __restrict__ out_w,
+                                   uint32_t* out_count) {
+  const uint32_t n = n_dev ? *n_dev : n_host;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = flags[n];
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const uint32_t o = flags[e];
+    if (flags[e + 1] == o) continue;
+    out_pos[o] = in_pos ? in_pos[e] : e;
+    out_cloud[o] = in_cloud ? in_cloud[e] : find_cloud(t.query_off, t.n_clouds, e);
+    out_w[o] = next_w[e];
   }
 }
 
 }  // namespace
+
+cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, const uint32_t* n_dev,
+                                    const CloudTables& t, const uint32_t* in_pos,
+                                    const uint32_t* in_cloud, const float* next_w,
+                                    uint32_t* out_pos, uint32_t* out_cloud, float* out_w,
+                                    uint32_t* out_count, int n_sms, cudaStream_t s) {
+  k_compact_fallback<<<n_sms * 8, 256, 0, s>>>(flags, n_host, n_dev, t, in_pos, in_cloud, next_w,
+                                               out_pos, out_cloud, out_w, out_count);
+  return cudaGetLastError();
+}
 
 size_t search_smem_bytes(uint32_t k, int warps_per_block) {
   return (size_t)warps_per_block * (512 + (size_t)k * 32 * 8);
