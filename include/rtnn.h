@@ -80,6 +80,8 @@ typedef struct rtnn_stats {
   float ms_total;            /* device time of the whole call (copies excluded) */
   uint32_t n_launches;       /* kernels of this library launched by the call */
   float ms_fallback;         /* the part of ms_search spent after the first pass */
+  uint64_t n_loaded;         /* candidate points streamed from HBM/L2 by all search passes */
+  uint64_t n_tested;         /* candidates distance-tested (each against 32 queries) */
 } rtnn_stats;
 
 typedef struct rtnn_ctx rtnn_ctx;

@@ -56,6 +56,7 @@ class Stats(ctypes.Structure):
         ("ms_build", ctypes.c_float), ("ms_partition", ctypes.c_float),
         ("ms_search", ctypes.c_float), ("ms_total", ctypes.c_float),
         ("n_launches", ctypes.c_uint32), ("ms_fallback", ctypes.c_float),
+        ("n_loaded", ctypes.c_uint64), ("n_tested", ctypes.c_uint64),
     ]
 
     def as_dict(self):

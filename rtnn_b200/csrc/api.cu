@@ -461,6 +461,8 @@ rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& 
     stats->grid_dims[1] = (uint32_t)c->h_grid->dy;
     stats->grid_dims[2] = (uint32_t)c->h_grid->dz;
     stats->n_launches = launches_of(sh, pr, false);
+    stats->n_loaded = h.n_loaded;
+    stats->n_tested = h.n_tested;
     if (timed) {
       cudaEventElapsedTime(&stats->ms_build, c->ev[0], c->ev[1]);
       cudaEventElapsedTime(&stats->ms_partition, c->ev[1], c->ev[2]);

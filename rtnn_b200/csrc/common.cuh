@@ -54,6 +54,8 @@ struct Counters {
   uint32_t total_cells;    // sum of cloud cells (written by k_grid_plan)
   uint32_t scan_tiles[24]; // dynamic tile counters, one per scan invocation
   uint32_t pad[3];
+  unsigned long long n_loaded;   // candidate points streamed by the search (all passes)
+  unsigned long long n_tested;   // candidates that passed the tile-box filter (x 32 lanes)
 };
 
 // Tables describing the clouds of one pipeline (all device arrays of n_clouds + 1).

@@ -143,6 +143,7 @@ k_search(SearchArgs a) {
       uint32_t n = 0;
       uint64_t root = ~0ull;
       float root_d = INFINITY;
+      uint32_t loaded = 0, tested = 0;   // work counters of this group (warp-uniform)
 
       for (int rb = 0; rb < nrows; rb += 32) {
         uint32_t rs = 0, re = 0;
@@ -173,6 +174,8 @@ k_search(SearchArgs a) {
             if (keep) stage[__popc(m & lt)] = p;
             __syncwarp();
             const int cnt = __popc(m);
+            loaded += min(32u, e0 - b);
+            tested += cnt;
             // 4. every lane against every staged point
             for (int c = 0; c < cnt; ++c) {
               const float4 cp = stage[c];
@@ -200,6 +203,10 @@ k_search(SearchArgs a) {
         }
       }
 
+      if (lane == 0 && loaded) {
+        atomicAdd(&a.ctr->n_loaded, (unsigned long long)loaded);
+        atomicAdd(&a.ctr->n_tested, (unsigned long long)tested);
+      }
       // completion: a narrowed search that found fewer than K neighbors is redone at r
       const bool incomplete = act && (lim_l < a.r2) && (n < k);
       const bool done = act && !incomplete;

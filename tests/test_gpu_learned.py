@@ -101,7 +101,8 @@ def _train(ctx, mode="knn", r=2.0, k=16, seeds=range(20, 26), epochs=15):
 def test_training_reduces_loss_and_learned_search_is_exact(ctx):
     import torch
     losses = _train(ctx)
-    assert losses[-1] < 0.7 * losses[0], losses
+    # normalised targets: predicting their mean scores 0.5; training must beat it and improve
+    assert losses[-1] < losses[0] and losses[-1] < 0.45, losses
     P = ctx.get_model()
     assert np.isfinite(P).all()
     p = _cloud(2, 60_000)
