@@ -43,6 +43,36 @@ __device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t i, uint32_t
   h[i * 32] = x;
 }
 
+constexpr uint32_t kPending = 8;   // per-lane hit buffer between heap updates
+
+// Moves every lane's pending hits into its heap (all lanes together, one hit each per
+// step). While the heap holds fewer than k entries hits are appended; at k it is
+// heapified (max-heap on (distance, index)) and later hits replace the root when smaller.
+__device__ __forceinline__ void flush_pending(uint64_t* heap, const uint64_t* pend, uint32_t& np,
+                                              uint32_t& n, uint32_t k, uint64_t& root,
+                                              float& root_d) {
+  const uint32_t steps = __reduce_max_sync(0xffffffffu, np);
+  for (uint32_t i = 0; i < steps; ++i) {
+    if (i < np) {
+      const uint64_t key = pend[i * 32];
+      if (n < k) {
+        heap[n * 32] = key;
+        ++n;
+        if (n == k) {
+          for (int j = (int)k / 2 - 1; j >= 0; --j) heap_sift_down(heap, j, k, heap[j * 32]);
+          root = heap[0];
+          root_d = __uint_as_float((uint32_t)(root >> 32));
+        }
+      } else if (key < root) {
+        heap_sift_down(heap, 0, k, key);
+        root = heap[0];
+        root_d = __uint_as_float((uint32_t)(root >> 32));
+      }
+    }
+  }
+  np = 0;
+}
+
 __device__ __forceinline__ float wmin(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -55,13 +85,15 @@ __device__ __forceinline__ float wmax(float v) {
 }
 
 template <bool KNN>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 k_search(SearchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   float4* stage = reinterpret_cast<float4*>(smem) + warp * 32;
-  uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * 512) + (size_t)warp * a.k * 32;
+  uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * 512) +
+                    (size_t)warp * (a.k + kPending) * 32;
   uint64_t* heap = heapw + lane;   // this lane's column: heap[i * 32]
+  uint64_t* pend = heapw + (size_t)a.k * 32 + lane;   // pending hits: pend[i * 32]
   const uint32_t lt = lanemask_lt();
   const uint32_t k = a.k;
   const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
@@ -143,6 +175,7 @@ k_search(SearchArgs a) {
       uint32_t n = 0;
       uint64_t root = ~0ull;
       float root_d = INFINITY;
+      uint32_t np = 0;                   // pending hits of this lane
       uint32_t loaded = 0, tested = 0;   // work counters of this group (warp-uniform)
 
       for (int rb = 0; rb < nrows; rb += 32) {
@@ -176,33 +209,26 @@ k_search(SearchArgs a) {
             const int cnt = __popc(m);
             loaded += min(32u, e0 - b);
             tested += cnt;
-            // 4. every lane against every staged point
+            // 4. every lane against every staged point; a hit only appends to the lane's
+            //    pending buffer, and the heaps are updated by the whole warp at once when
+            //    some lane's buffer is full (no per-candidate divergence on heap work)
             for (int c = 0; c < cnt; ++c) {
               const float4 cp = stage[c];
               const float d = dist2_ref(q.x, q.y, q.z, cp.x, cp.y, cp.z);
               const bool hit = (d < lim_l) && (!KNN || d > 0.f) && (d <= root_d);
               if (hit) {
-                const uint64_t key = ((uint64_t)__float_as_uint(d) << 32) | __float_as_uint(cp.w);
-                if (n < k) {
-                  heap[n * 32] = key;
-                  ++n;
-                  if (n == k) {
-                    for (int i = (int)k / 2 - 1; i >= 0; --i) heap_sift_down(heap, i, k, heap[i * 32]);
-                    root = heap[0];
-                    root_d = __uint_as_float((uint32_t)(root >> 32));
-                  }
-                } else if (key < root) {
-                  heap_sift_down(heap, 0, k, key);
-                  root = heap[0];
-                  root_d = __uint_as_float((uint32_t)(root >> 32));
-                }
+                pend[np * 32] = ((uint64_t)__float_as_uint(d) << 32) | __float_as_uint(cp.w);
+                ++np;
               }
+              if (__any_sync(0xffffffffu, np == kPending))
+                flush_pending(heap, pend, np, n, k, root, root_d);
             }
             __syncwarp();
           }
         }
       }
 
+      flush_pending(heap, pend, np, n, k, root, root_d);
       if (lane == 0 && loaded) {
         atomicAdd(&a.ctr->n_loaded, (unsigned long long)loaded);
         atomicAdd(&a.ctr->n_tested, (unsigned long long)tested);
@@ -278,7 +304,7 @@ cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, cons
 }
 
 size_t search_smem_bytes(uint32_t k, int warps_per_block) {
-  return (size_t)warps_per_block * (512 + (size_t)k * 32 * 8);
+  return (size_t)warps_per_block * (512 + (size_t)(k + kPending) * 32 * 8);
 }
 
 cudaError_t search_prepare(int device) {
