@@ -44,6 +44,26 @@ __device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t i, uint32_t
 }
 
 constexpr uint32_t kPending = 8;   // per-lane hit buffer between heap updates
+constexpr int kCheck = 4;          // candidates tested between two buffer-full votes
+constexpr int kStage = 64;         // staged candidates per warp (float4)
+
+// Hit window on the bits of a non-negative FP32 distance d (bit order == value order):
+// radius: d < lim;  KNN: 0 < d < lim;  and, once the heap is full, d <= root distance
+// (equal distances may still win on index). A hit is bits(d) - lo <= span (unsigned);
+// an inactive lane gets a window that no sum of squares can hit (-0.0 only).
+__device__ __forceinline__ void hit_window(bool active, float lim, float root_d, bool knn,
+                                           uint32_t& lo, uint32_t& span) {
+  const uint32_t l = knn ? 1u : 0u;
+  uint32_t h = __float_as_uint(root_d);
+  if (lim > 0.f) h = min(h, __float_as_uint(lim) - 1u);
+  if (!active || !(lim > 0.f) || h < l) {
+    lo = 0x80000000u;
+    span = 0u;
+  } else {
+    lo = l;
+    span = h - l;
+  }
+}
 
 // Moves every lane's pending hits into its heap (all lanes together, one hit each per
 // step). While the heap holds fewer than k entries hits are appended; at k it is
@@ -89,8 +109,8 @@ __global__ void __launch_bounds__(256, 2)
 k_search(SearchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  float4* stage = reinterpret_cast<float4*>(smem) + warp * 32;
-  uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * 512) +
+  float4* stage = reinterpret_cast<float4*>(smem) + warp * kStage;
+  uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * kStage * 16) +
                     (size_t)warp * (a.k + kPending) * 32;
   uint64_t* heap = heapw + lane;   // this lane's column: heap[i * 32]
   uint64_t* pend = heapw + (size_t)a.k * 32 + lane;   // pending hits: pend[i * 32]
@@ -177,6 +197,27 @@ k_search(SearchArgs a) {
       float root_d = INFINITY;
       uint32_t np = 0;                   // pending hits of this lane
       uint32_t loaded = 0, tested = 0;   // work counters of this group (warp-uniform)
+      // hit test on the distance bits: lo <= bits(d) <= lo + span (see hit_window)
+      uint32_t wlo, wspan;
+      hit_window(act, lim_l, root_d, KNN, wlo, wspan);
+
+      // 4. every lane against a staged point; a hit only appends to the lane's pending
+      //    buffer, and the heaps are updated by the whole warp at once once some lane
+      //    holds more than kPending - kCheck hits (checked every kCheck candidates)
+      auto test = [&](const float4 cp) {
+        const float d = dist2_ref(q.x, q.y, q.z, cp.x, cp.y, cp.z);
+        if (__float_as_uint(d) - wlo <= wspan) {
+          pend[np * 32] = ((uint64_t)__float_as_uint(d) << 32) | __float_as_uint(cp.w);
+          ++np;
+        }
+      };
+      auto check = [&]() {
+        if (__any_sync(0xffffffffu, np > kPending - kCheck)) {
+          flush_pending(heap, pend, np, n, k, root, root_d);
+          hit_window(act, lim_l, root_d, KNN, wlo, wspan);
+        }
+      };
+      uint32_t sc = 0;   // staged candidates (warp-uniform, < 32 between batches)
 
       for (int rb = 0; rb < nrows; rb += 32) {
         uint32_t rs = 0, re = 0;
@@ -192,7 +233,8 @@ k_search(SearchArgs a) {
           const uint32_t s0 = __shfl_sync(0xffffffffu, rs, j);
           const uint32_t e0 = __shfl_sync(0xffffffffu, re, j);
           for (uint32_t b = s0; b < e0; b += 32) {
-            // 3. stream 32 points, drop those farther than R from the box, compact
+            // 3. stream 32 points, drop those farther than R from the box, compact the
+            //    survivors behind the ones already staged (rows accumulate)
             const uint32_t idx = b + lane;
             bool keep = false;
             float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -204,29 +246,32 @@ k_search(SearchArgs a) {
               keep = ex * ex + ey * ey + ez * ez <= R2k;
             }
             const uint32_t m = __ballot_sync(0xffffffffu, keep);
-            if (keep) stage[__popc(m & lt)] = p;
-            __syncwarp();
-            const int cnt = __popc(m);
+            if (keep) stage[sc + __popc(m & lt)] = p;
+            sc += __popc(m);
             loaded += min(32u, e0 - b);
-            tested += cnt;
-            // 4. every lane against every staged point; a hit only appends to the lane's
-            //    pending buffer, and the heaps are updated by the whole warp at once when
-            //    some lane's buffer is full (no per-candidate divergence on heap work)
-            for (int c = 0; c < cnt; ++c) {
-              const float4 cp = stage[c];
-              const float d = dist2_ref(q.x, q.y, q.z, cp.x, cp.y, cp.z);
-              const bool hit = (d < lim_l) && (!KNN || d > 0.f) && (d <= root_d);
-              if (hit) {
-                pend[np * 32] = ((uint64_t)__float_as_uint(d) << 32) | __float_as_uint(cp.w);
-                ++np;
+            tested += __popc(m);
+            if (sc >= 32) {
+              __syncwarp();
+#pragma unroll
+              for (int c0 = 0; c0 < 32; c0 += kCheck) {
+#pragma unroll
+                for (int c = c0; c < c0 + kCheck; ++c) test(stage[c]);
+                check();
               }
-              if (__any_sync(0xffffffffu, np == kPending))
-                flush_pending(heap, pend, np, n, k, root, root_d);
+              __syncwarp();
+              sc -= 32;
+              if (lane < sc) stage[lane] = stage[32 + lane];
+              __syncwarp();
             }
-            __syncwarp();
           }
         }
       }
+      __syncwarp();
+      for (uint32_t c0 = 0; c0 < sc; c0 += kCheck) {
+        for (uint32_t c = c0; c < min(c0 + kCheck, sc); ++c) test(stage[c]);
+        check();
+      }
+      __syncwarp();
 
       flush_pending(heap, pend, np, n, k, root, root_d);
       if (lane == 0 && loaded) {
@@ -304,7 +349,7 @@ cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, cons
 }
 
 size_t search_smem_bytes(uint32_t k, int warps_per_block) {
-  return (size_t)warps_per_block * (512 + (size_t)(k + kPending) * 32 * 8);
+  return (size_t)warps_per_block * (kStage * 16 + (size_t)(k + kPending) * 32 * 8);
 }
 
 cudaError_t search_prepare(int device) {
