@@ -204,12 +204,22 @@ k_search(SearchArgs a) {
       // 4. every lane against a staged point; a hit only appends to the lane's pending
       //    buffer, and the heaps are updated by the whole warp at once once some lane
       //    holds more than kPending - kCheck hits (checked every kCheck candidates)
-      auto test = [&](const float4 cp) {
-        const float d = dist2_ref(q.x, q.y, q.z, cp.x, cp.y, cp.z);
-        if (__float_as_uint(d) - wlo <= wspan) {
-          pend[np * 32] = ((uint64_t)__float_as_uint(d) << 32) | __float_as_uint(cp.w);
-          ++np;
-        }
+      // four candidates at a time: loads first, four independent distance chains, then
+      // branch-free appends (the slot is always written, the count moves on a hit only)
+      auto test4 = [&](int c0) {
+        const float4 p0 = stage[c0], p1 = stage[c0 + 1], p2 = stage[c0 + 2], p3 = stage[c0 + 3];
+        const float d0 = dist2_ref(q.x, q.y, q.z, p0.x, p0.y, p0.z);
+        const float d1 = dist2_ref(q.x, q.y, q.z, p1.x, p1.y, p1.z);
+        const float d2 = dist2_ref(q.x, q.y, q.z, p2.x, p2.y, p2.z);
+        const float d3 = dist2_ref(q.x, q.y, q.z, p3.x, p3.y, p3.z);
+        pend[np * 32] = ((uint64_t)__float_as_uint(d0) << 32) | __float_as_uint(p0.w);
+        np += (__float_as_uint(d0) - wlo <= wspan) ? 1u : 0u;
+        pend[np * 32] = ((uint64_t)__float_as_uint(d1) << 32) | __float_as_uint(p1.w);
+        np += (__float_as_uint(d1) - wlo <= wspan) ? 1u : 0u;
+        pend[np * 32] = ((uint64_t)__float_as_uint(d2) << 32) | __float_as_uint(p2.w);
+        np += (__float_as_uint(d2) - wlo <= wspan) ? 1u : 0u;
+        pend[np * 32] = ((uint64_t)__float_as_uint(d3) << 32) | __float_as_uint(p3.w);
+        np += (__float_as_uint(d3) - wlo <= wspan) ? 1u : 0u;
       };
       auto check = [&]() {
         if (__any_sync(0xffffffffu, np > kPending - kCheck)) {
@@ -254,8 +264,7 @@ k_search(SearchArgs a) {
               __syncwarp();
 #pragma unroll
               for (int c0 = 0; c0 < 32; c0 += kCheck) {
-#pragma unroll
-                for (int c = c0; c < c0 + kCheck; ++c) test(stage[c]);
+                test4(c0);
                 check();
               }
               __syncwarp();
@@ -266,12 +275,16 @@ k_search(SearchArgs a) {
           }
         }
       }
-      __syncwarp();
-      for (uint32_t c0 = 0; c0 < sc; c0 += kCheck) {
-        for (uint32_t c = c0; c < min(c0 + kCheck, sc); ++c) test(stage[c]);
-        check();
+      if (sc > 0) {
+        // pad the last batch with points at infinity: their distance never passes
+        if (lane >= sc) stage[lane] = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+        __syncwarp();
+        for (uint32_t c0 = 0; c0 < sc; c0 += kCheck) {
+          test4((int)c0);
+          check();
+        }
+        __syncwarp();
       }
-      __syncwarp();
 
       flush_pending(heap, pend, np, n, k, root, root_d);
       if (lane == 0 && loaded) {
