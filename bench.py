@@ -284,7 +284,7 @@ def run_rtnn(args, rank, world):
     ctx = rtnn_b200.Context(dev)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
-    model_info = train_model(ctx, cfg, args.scale, rank)
+    base_tuning = ctx.tuning().as_dict()
 
     tp = torch.from_numpy(cfg["points"]).cuda()
     tq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).cuda()
@@ -319,24 +319,35 @@ def run_rtnn(args, rank, world):
         return max_over_ranks(e0.elapsed_time(e1) / steps), ck
 
     common = dict(mode=cfg["mode"], radius=cfg["radius"], k=K)
+    from rtnn_b200 import autotune as at
+    wl_args = (tp, cfg["offsets"], tq, cfg["qoffsets"])
+
+    # the plain grid search (full radius for every query), with its own best tuning
+    plain_ms, plain_tuning, result_plain = None, None, None
+    if not args.no_plain:
+        plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, use_cache=False, **common)
+        plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
+        plain_ms, _ = timed(plain, args.steps, max(1, args.warmup // 2))
+        plain.execute(tp, tq, out)
+        result_plain = _row_sets(out)
+        plain.close()
+
+    # learned partition: grid knobs tuned on the analytic partition, the width model
+    # trained on clouds of other seeds at that tuning, then margin / fallback passes
+    ctx.set_tuning(**base_tuning)
+    at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, partition=True, use_cache=False, **common)
+    model_info = train_model(ctx, cfg, args.scale, rank)
+    learned_tuning = at.autotune(ctx, *wl_args, knobs=at.LEARNED_KNOBS, learned=True,
+                                 use_cache=False, **common)
     learned = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=True, **common)
     ms_learned, clocks = timed(learned, args.steps, args.warmup, ClockSampler(dev))
     st = rtnn_b200.Stats()
     learned.execute(tp, tq, out, stats=st)
     launches_per_step = st.n_launches
     fallback = st.n_fallback
-    result_learned = out.clone()
     learned.close()
-
-    plain_ms = None
-    if not args.no_plain:
-        plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
-        plain_ms, _ = timed(plain, args.steps, max(1, args.warmup // 2))
-        plain.execute(tp, tq, out)
-        identical = bool(torch.equal(_row_sets(out), _row_sets(result_learned)))
-        plain.close()
-    else:
-        identical = None
+    identical = None if result_plain is None else bool(torch.equal(_row_sets(out), result_plain))
+    del result_plain
 
     # dominant kernel (search, both passes) timed with the library's events on `stream`
     nog = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=False, **common)
@@ -394,7 +405,8 @@ def run_rtnn(args, rank, world):
             "identical_sets": identical, "fallback_queries": int(fallback),
             "stage_ms": {"build": round(statistics.mean(ms_build), 3),
                          "partition": round(statistics.mean(ms_part), 3), "search": round(ms_s, 3)},
-            "model": model_info, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "model": model_info, "tuning": {"learned": learned_tuning, "plain": plain_tuning},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches_per_step * args.steps), "clocks": clocks}
     if rank == 0:
         print(json.dumps(line), flush=True)
