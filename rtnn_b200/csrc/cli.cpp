@@ -176,7 +176,7 @@ int main(int argc, char** argv) {
   if (o.parse_only) {
     double sum = 0;
     for (float v : P) sum += v;
-    std::printf("points %llu checksum %.9g\n", (unsigned long long)np, sum);
+    std::printf("points %llu checksum %.17g\n", (unsigned long long)np, sum);
     return 0;
   }
   if (np == 0 || nq == 0) {
