@@ -162,6 +162,28 @@ typedef struct rtnn_tuning {
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);
 rtnn_status rtnn_set_tuning(rtnn_ctx* ctx, const rtnn_tuning* tuning);
 
+/* Search for callers that cannot allocate device memory. It has no counterpart in the
+ * reference. For hosts that own all device memory through
+ * their own pool, real-time loops that cannot afford cudaMalloc's implicit synchronisation,
+ * and code running while a CUDA graph is captured in global mode: this call makes no
+ * cudaMalloc, cudaFree or other allocation, and needs no context.
+ * Plain (unpartitioned) radius or KNN search, the same rows as rtnn_search with flags 0.
+ * Device pointers only; `stream` is a cudaStream_t (NULL: the legacy default stream); the
+ * call returns after the search has finished. Its scratch is one fixed array of
+ * RTNN_NOALLOC_SCRATCH_BYTES in device memory, held by every GPU that loads the library
+ * until the process exits, and shared by all calls: calls whose work overlaps on the GPU
+ * race and must be serialised by the caller. Limits: at most RTNN_NOALLOC_MAX_POINTS points
+ * and RTNN_NOALLOC_MAX_QUERIES queries (RTNN_ERR_INVALID_ARGUMENT otherwise). The first call
+ * on a device looks up the array's device address and should come before any stream
+ * capture. errbuf (optional, errlen bytes) receives a message when the call fails. */
+#define RTNN_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define RTNN_NOALLOC_MAX_POINTS (1u << 18)
+#define RTNN_NOALLOC_MAX_QUERIES (1u << 18)
+rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_points,
+                                const float* d_queries, uint32_t n_queries, rtnn_mode mode,
+                                float radius, uint32_t k, int32_t* d_out, void* stream,
+                                char* errbuf, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,7 +23,8 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
            "-Xptxas", "-O3", "-I" + INCLUDE, "-I" + CSRC]
-SOURCES = ["scan.cu", "radix_sort.cu", "build_grid.cu", "search.cu", "partition.cu", "api.cu"]
+SOURCES = ["scan.cu", "radix_sort.cu", "build_grid.cu", "search.cu", "partition.cu", "api.cu",
+           "noalloc.cu"]
 
 
 def _headers():
