@@ -49,7 +49,36 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="train the width model, then run one learned step (no graph) between "
+                         "cudaProfilerStart/Stop, for ncu --profile-from-start off; no JSON line")
     return ap.parse_args()
+
+
+def run_profile(args):
+    """One learned step of the workload bracketed by cudaProfilerStart/Stop."""
+    import torch
+    import rtnn_b200
+    cfg = make_workload(args.workload, args.scale, 0)
+    ctx = rtnn_b200.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    ctx.set_tuning(points_per_cell=1.0, width_margin=1.3, fallback_passes=4)
+    train_model(ctx, cfg, args.scale, 0)
+    tp = torch.from_numpy(cfg["points"]).cuda()
+    tq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).cuda()
+    out = torch.empty((cfg["n_queries"], cfg["k"]), dtype=torch.int32, device="cuda")
+    plan = ctx.plan(cfg["offsets"], cfg["qoffsets"], mode=cfg["mode"], radius=cfg["radius"],
+                    k=cfg["k"], learned=True, use_graph=False)
+    plan.execute(tp, tq, out)
+    torch.cuda.synchronize()
+    st = rtnn_b200.Stats()
+    torch.cuda.profiler.start()
+    plan.execute(tp, tq, out, stats=st)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print("profiled step:", json.dumps(st.as_dict()), flush=True)
+    plan.close()
+    ctx.close()
 
 
 # ---------------------------------------------------------------------------------------
@@ -428,7 +457,9 @@ def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_rtnn(args, rank, world)
