@@ -68,9 +68,11 @@ __device__ __forceinline__ void hit_window(bool active, float lim, float root_d,
 // Moves every lane's pending hits into its heap (all lanes together, one hit each per
 // step). While the heap holds fewer than k entries hits are appended; at k it is
 // heapified (max-heap on (distance, index)) and later hits replace the root when smaller.
-__device__ __forceinline__ void flush_pending(uint64_t* heap, const uint64_t* pend, uint32_t& np,
-                                              uint32_t& n, uint32_t k, uint64_t& root,
-                                              float& root_d) {
+// Kept out of line: it is reached from several places of the test loop, and one copy keeps
+// the search kernel's hot loop small enough for the instruction cache.
+__device__ __noinline__ void flush_pending(uint64_t* heap, const uint64_t* pend, uint32_t& np,
+                                           uint32_t& n, uint32_t k, uint64_t& root,
+                                           float& root_d) {
   const uint32_t steps = __reduce_max_sync(0xffffffffu, np);
   for (uint32_t i = 0; i < steps; ++i) {
     if (i < np) {
@@ -262,7 +264,7 @@ k_search(SearchArgs a) {
             tested += __popc(m);
             if (sc >= 32) {
               __syncwarp();
-#pragma unroll
+#pragma unroll 2
               for (int c0 = 0; c0 < 32; c0 += kCheck) {
                 test4(c0);
                 check();
