@@ -159,10 +159,12 @@ rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32
 }
 
 void finish_shapes(Shapes& sh, const rtnn_tuning& tu) {
-  uint32_t mb = (ceil_log2(std::max<uint64_t>(sh.max_cloud_q, 2)) + 2) / 3;
-  mb = std::max(1u, std::min(10u, mb));
+  // Morton steps per axis: about 64 key cells per query of the largest cloud
+  uint32_t mb = (ceil_log2(std::max<uint64_t>(sh.max_cloud_q, 2)) + 6 + 2) / 3;
+  mb = std::max(1u, std::min(16u, mb));
   const uint32_t cb = ceil_log2(sh.n_clouds);
   if (cb + 3 * mb + 4 > 64) mb = (60 - cb) / 3;   // room for 4 density-bucket bits
+  if (mb > 1 && cb + 3 * mb + 4 > 32 && cb + 3 * (mb - 1) + 4 <= 32) --mb;   // stay 32-bit
   sh.morton_bits = mb;
   sh.key_bits = std::max(8u, cb + 3 * mb);
   sh.key64 = sh.key_bits > 32;

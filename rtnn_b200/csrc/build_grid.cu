@@ -175,10 +175,10 @@ k_grid_plan(CloudTables t, const uint32_t* __restrict__ bbox, float radius, floa
       g.cell = cell; g.inv_cell = 1.0f / cell;
       g.dx = d[0]; g.dy = d[1]; g.dz = d[2];
       g.n_cells = (uint32_t)((uint64_t)d[0] * d[1] * d[2]);
-      int maxd = max(d[0], max(d[1], d[2]));
-      uint32_t bits = 0;
-      while ((1 << bits) < maxd) ++bits;
-      g.morton_shift = bits > morton_bits ? bits - morton_bits : 0;
+      // query order: Morton code on 2^morton_bits steps across the cloud's longest side
+      // (finer than the cells, so dense cells still yield compact 32-query tiles)
+      const float ext = fmaxf(fmaxf(mx[0] - mn[0], mx[1] - mn[1]), fmaxf(mx[2] - mn[2], 1e-30f));
+      g.morton_scale = (float)((1u << morton_bits) - 1u) / ext;
       ncell = g.n_cells;
     }
     // block-wide exclusive scan of ncell (values < 2^32, carry kept in 64 bits)
@@ -291,12 +291,12 @@ k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
   const ChunkRange r = chunk_range(t.qchunk_base, t.query_off, t.n_clouds, blockIdx.x);
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
   const CloudGrid g = grids[r.cloud];
+  const int top = (int)((1u << morton_bits) - 1u);
   for (uint32_t i = threadIdx.x; i < r.end - r.begin; i += blockDim.x) {
-    const int cx = clamp_cell(cell_coord_f(s_xyz[3 * i], g.ox, g.inv_cell), g.dx);
-    const int cy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.inv_cell), g.dy);
-    const int cz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.inv_cell), g.dz);
-    const uint32_t m = morton3((uint32_t)cx >> g.morton_shift, (uint32_t)cy >> g.morton_shift,
-                               (uint32_t)cz >> g.morton_shift);
+    const int fx = clamp_cell(cell_coord_f(s_xyz[3 * i], g.ox, g.morton_scale), top + 1);
+    const int fy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.morton_scale), top + 1);
+    const int fz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.morton_scale), top + 1);
+    const uint64_t m = morton3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz);
     const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits) : 0u;
     keys[r.begin + i] = ((KeyT)r.cloud << (3 * morton_bits + level_bits)) |
                         ((KeyT)lvl << (3 * morton_bits)) | (KeyT)m;

@@ -40,7 +40,7 @@ struct __align__(16) CloudGrid {
   float inv_cell;        // 1 / cell
   int dx, dy, dz;        // cells per axis
   uint32_t cell_base;    // first cell of this cloud in the global cell array
-  uint32_t morton_shift; // cell coords >> shift before Morton interleaving
+  float morton_scale;    // query order: Morton code of floor((x - origin) * morton_scale)
   uint32_t n_cells;      // dx * dy * dz
   uint32_t pad;
 };
@@ -127,6 +127,20 @@ __device__ __forceinline__ uint32_t spread3(uint32_t x) {
 }
 __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+
+// 21-bit-per-axis Morton interleave into 64 bits (same bit convention).
+__device__ __forceinline__ uint64_t spread3_64(uint64_t x) {
+  x &= 0x1fffffull;
+  x = (x | (x << 32)) & 0x001f00000000ffffull;
+  x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+  x = (x | (x << 8)) & 0x100f00f00f00f00full;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+  x = (x | (x << 2)) & 0x1249249249249249ull;
+  return x;
+}
+__device__ __forceinline__ uint64_t morton3_64(uint32_t x, uint32_t y, uint32_t z) {
+  return spread3_64(x) | (spread3_64(y) << 1) | (spread3_64(z) << 2);
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
