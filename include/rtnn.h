@@ -157,6 +157,9 @@ typedef struct rtnn_tuning {
   float width_margin;     /* learned width = margin * predicted K-th distance */
   uint32_t fallback_passes;   /* partitioned search: passes that retry short queries at twice
                                  their width before the last pass at the full radius (0..6) */
+  float lane_walk_ratio;      /* a 32-query tile whose extent exceeds ratio x its search width
+                                 is searched lane by lane (each lane walks its own query's
+                                 cells) instead of sharing one candidate stream; 0: never */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

@@ -36,6 +36,7 @@ struct SearchArgs {
   uint32_t k;
   uint32_t flags;              // kSearch*
   int pass;                    // kPassMain, kPassEscalate or kPassFinal
+  float lane_walk_ratio;       // tile spread > ratio * width: per-lane walk (0: never)
 };
 constexpr int kPassMain = 0;      // sorted queries, widths from the partition
 constexpr int kPassEscalate = 1;  // fallback list at its (doubled) widths

@@ -208,8 +208,7 @@ k_search(SearchArgs a) {
       //    holds more than kPending - kCheck hits (checked every kCheck candidates)
       // four candidates at a time: loads first, four independent distance chains, then
       // branch-free appends (the slot is always written, the count moves on a hit only)
-      auto test4 = [&](int c0) {
-        const float4 p0 = stage[c0], p1 = stage[c0 + 1], p2 = stage[c0 + 2], p3 = stage[c0 + 3];
+      auto test4 = [&](const float4 p0, const float4 p1, const float4 p2, const float4 p3) {
         const float d0 = dist2_ref(q.x, q.y, q.z, p0.x, p0.y, p0.z);
         const float d1 = dist2_ref(q.x, q.y, q.z, p1.x, p1.y, p1.z);
         const float d2 = dist2_ref(q.x, q.y, q.z, p2.x, p2.y, p2.z);
@@ -230,8 +229,64 @@ k_search(SearchArgs a) {
         }
       };
       uint32_t sc = 0;   // staged candidates (warp-uniform, < 32 between batches)
+      // Tiles whose queries spread far beyond their width (dense clouds, narrow widths)
+      // walk per lane: each lane visits only the cells of its own query's box, so it tests
+      // a few times K points instead of everything near the whole tile.
+      const float spread = fmaxf(fmaxf(bx1 - bx0, by1 - by0), bz1 - bz0);
+      const bool lane_walk = a.lane_walk_ratio > 0.f && spread > a.lane_walk_ratio * R;
 
-      for (int rb = 0; rb < nrows; rb += 32) {
+      if (lane_walk) {
+        const float INF = INFINITY;
+        const float4 far = make_float4(INF, INF, INF, 0.f);
+        int l0 = 0, h0 = -1, l1 = 0, h1 = -1, l2 = 0, h2 = -1;
+        if (act && grid_ok) {
+          const float Rl = __fmul_ru(w, 1.000001f);
+          const float gx0 = cell_coord_f(__fsub_rn(q.x, Rl), g.ox, g.inv_cell);
+          const float gx1 = cell_coord_f(__fadd_rn(q.x, Rl), g.ox, g.inv_cell);
+          const float gy0 = cell_coord_f(__fsub_rn(q.y, Rl), g.oy, g.inv_cell);
+          const float gy1 = cell_coord_f(__fadd_rn(q.y, Rl), g.oy, g.inv_cell);
+          const float gz0 = cell_coord_f(__fsub_rn(q.z, Rl), g.oz, g.inv_cell);
+          const float gz1 = cell_coord_f(__fadd_rn(q.z, Rl), g.oz, g.inv_cell);
+          if (gx0 <= (float)(g.dx - 1) && gx1 >= 0.f && gy0 <= (float)(g.dy - 1) && gy1 >= 0.f &&
+              gz0 <= (float)(g.dz - 1) && gz1 >= 0.f) {
+            l0 = (int)fmaxf(gx0, 0.f); h0 = (int)fminf(gx1, (float)(g.dx - 1));
+            l1 = (int)fmaxf(gy0, 0.f); h1 = (int)fminf(gy1, (float)(g.dy - 1));
+            l2 = (int)fmaxf(gz0, 0.f); h2 = (int)fminf(gz1, (float)(g.dz - 1));
+          }
+        }
+        const int nyl = h1 - l1 + 1;
+        const int nrl = (h0 >= l0 && h1 >= l1 && h2 >= l2) ? nyl * (h2 - l2 + 1) : 0;
+        int ri = 0;
+        uint32_t ptr = 0, end = 0, mine = 0;
+        while (true) {
+          while (ptr >= end && ri < nrl) {   // next non-empty row of this lane's box
+            const int cy = l1 + ri % nyl, cz = l2 + ri / nyl;
+            const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+            ptr = __ldg(a.cells + rowc + l0);
+            end = __ldg(a.cells + rowc + h0 + 1);
+            ++ri;
+          }
+          if (!__any_sync(0xffffffffu, ptr < end)) break;
+          // four points of this lane's current row; past its end, points at infinity
+          const float4 p0 = ptr < end ? __ldg(a.spts + ptr) : far;
+          const float4 p1 = ptr + 1 < end ? __ldg(a.spts + ptr + 1) : far;
+          const float4 p2 = ptr + 2 < end ? __ldg(a.spts + ptr + 2) : far;
+          const float4 p3 = ptr + 3 < end ? __ldg(a.spts + ptr + 3) : far;
+          const uint32_t took = min(end - ptr, 4u);
+          mine += took;
+          ptr += took;
+          test4(p0, p1, p2, p3);
+          check();
+        }
+        // counters in units of 32 lane-tests, like one staged point of the shared walk
+        uint32_t sum = mine;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        loaded += sum;
+        tested += (sum + 31) / 32;
+      }
+
+      for (int rb = 0; rb < (lane_walk ? 0 : nrows); rb += 32) {
         uint32_t rs = 0, re = 0;
         const int ri = rb + lane;
         if (ri < nrows) {
@@ -266,7 +321,7 @@ k_search(SearchArgs a) {
               __syncwarp();
 #pragma unroll 2
               for (int c0 = 0; c0 < 32; c0 += kCheck) {
-                test4(c0);
+                test4(stage[c0], stage[c0 + 1], stage[c0 + 2], stage[c0 + 3]);
                 check();
               }
               __syncwarp();
@@ -282,7 +337,7 @@ k_search(SearchArgs a) {
         if (lane >= sc) stage[lane] = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
         __syncwarp();
         for (uint32_t c0 = 0; c0 < sc; c0 += kCheck) {
-          test4((int)c0);
+          test4(stage[c0], stage[c0 + 1], stage[c0 + 2], stage[c0 + 3]);
           check();
         }
         __syncwarp();

@@ -267,3 +267,22 @@ def test_fp64_disagreement_is_only_boundary_pairs(ctx):
             b = set(ref64[qi][ref64[qi] >= 0].tolist())
             diff |= {(qi, x) for x in a ^ b}
         assert diff == pairs
+
+
+@pytest.mark.parametrize("ratio", [0.0, 0.01, 1.0, 1e9])
+def test_walk_modes_give_identical_rows(ctx, ratio):
+    """Shared candidate stream (ratio 0 or huge) and per-lane walk (tiny ratio) agree
+    with the oracle row for row, in every mode and with the partition on."""
+    base = ctx.tuning().as_dict()
+    try:
+        ctx.set_tuning(**{**base, "lane_walk_ratio": ratio})
+        p, off = wl.multicloud(n_clouds=24, lo=64, hi=6000, seed=9)
+        got = ctx.search_batched(p, off, mode="knn", radius=0.2, k=32, sorted_rows=True,
+                                 partition=True)
+        assert np.array_equal(got, oracle.grid_search_batched(p, off, mode="knn", r=0.2, k=32))
+        u = wl.uniform_cube(30_000, 40.0, seed=4)
+        for mode in ("radius", "knn"):
+            got = ctx.search(u, None, mode, 3.0, 40, sorted_rows=True)
+            assert np.array_equal(got, oracle.grid_search(u, None, mode, 3.0, 40))
+    finally:
+        ctx.set_tuning(**base)
