@@ -43,6 +43,50 @@ __device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t i, uint32_t
   h[i * 32] = x;
 }
 
+// ---- packed FP32x2 arithmetic (sm_100a): two IEEE round-to-nearest operations per
+//      instruction, each element rounded on its own exactly like __fsub_rn / __fmul_rn /
+//      __fadd_rn, so two candidates' distances cost one instruction chain
+__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk2(uint64_t v, uint32_t& lo, uint32_t& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+// dist2_ref of two points at once: ((dx*dx + dy*dy) + dz*dz), every step rounded
+__device__ __forceinline__ uint64_t dist2_pair(uint64_t qx, uint64_t qy, uint64_t qz, uint64_t px,
+                                               uint64_t py, uint64_t pz) {
+  const uint64_t dx = sub2(qx, px), dy = sub2(qy, py), dz = sub2(qz, pz);
+  return add2(add2(mul2(dx, dx), mul2(dy, dy)), mul2(dz, dz));
+}
+
+// Staged candidates are kept in pairs, {x0 x1 y0 y1 | z0 z1 w0 w1} (32 bytes per two
+// slots), so two 16-byte loads give two candidates already packed for the f32x2 math.
+__device__ __forceinline__ void stage_put(float* st, uint32_t slot, float4 p) {
+  float* b = st + (slot >> 1) * 8 + (slot & 1);
+  b[0] = p.x; b[2] = p.y; b[4] = p.z; b[6] = p.w;
+}
+__device__ __forceinline__ float4 stage_get(const float* st, uint32_t slot) {
+  const float* b = st + (slot >> 1) * 8 + (slot & 1);
+  return make_float4(b[0], b[2], b[4], b[6]);
+}
+
 constexpr uint32_t kPending = 8;   // per-lane hit buffer between heap updates
 constexpr int kCheck = 4;          // candidates tested between two buffer-full votes
 constexpr int kStage = 64;         // staged candidates per warp (float4)
@@ -111,7 +155,7 @@ __global__ void __launch_bounds__(256, 2)
 k_search(SearchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  float4* stage = reinterpret_cast<float4*>(smem) + warp * kStage;
+  float* stage = reinterpret_cast<float*>(smem) + warp * kStage * 4;   // pair layout
   uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * kStage * 16) +
                     (size_t)warp * (a.k + kPending) * 32;
   uint64_t* heap = heapw + lane;   // this lane's column: heap[i * 32]
@@ -208,19 +252,31 @@ k_search(SearchArgs a) {
       //    holds more than kPending - kCheck hits (checked every kCheck candidates)
       // four candidates at a time: loads first, four independent distance chains, then
       // branch-free appends (the slot is always written, the count moves on a hit only)
+      const uint64_t qx2 = pk2(q.x, q.x), qy2 = pk2(q.y, q.y), qz2 = pk2(q.z, q.z);
+      auto test_pair = [&](uint64_t px, uint64_t py, uint64_t pz, uint32_t i0, uint32_t i1) {
+        uint32_t d0, d1;
+        upk2(dist2_pair(qx2, qy2, qz2, px, py, pz), d0, d1);
+        pend[np * 32] = ((uint64_t)d0 << 32) | i0;
+        np += (d0 - wlo <= wspan) ? 1u : 0u;
+        pend[np * 32] = ((uint64_t)d1 << 32) | i1;
+        np += (d1 - wlo <= wspan) ? 1u : 0u;
+      };
+      // four staged candidates (slots c0..c0+3, c0 even): two pairs, two f32x2 chains
+      auto test4_staged = [&](int c0) {
+        const float4 a0 = *reinterpret_cast<const float4*>(stage + (c0 >> 1) * 8);
+        const float4 b0 = *reinterpret_cast<const float4*>(stage + (c0 >> 1) * 8 + 4);
+        const float4 a1 = *reinterpret_cast<const float4*>(stage + (c0 >> 1) * 8 + 8);
+        const float4 b1 = *reinterpret_cast<const float4*>(stage + (c0 >> 1) * 8 + 12);
+        test_pair(pk2(a0.x, a0.y), pk2(a0.z, a0.w), pk2(b0.x, b0.y), __float_as_uint(b0.z),
+                  __float_as_uint(b0.w));
+        test_pair(pk2(a1.x, a1.y), pk2(a1.z, a1.w), pk2(b1.x, b1.y), __float_as_uint(b1.z),
+                  __float_as_uint(b1.w));
+      };
       auto test4 = [&](const float4 p0, const float4 p1, const float4 p2, const float4 p3) {
-        const float d0 = dist2_ref(q.x, q.y, q.z, p0.x, p0.y, p0.z);
-        const float d1 = dist2_ref(q.x, q.y, q.z, p1.x, p1.y, p1.z);
-        const float d2 = dist2_ref(q.x, q.y, q.z, p2.x, p2.y, p2.z);
-        const float d3 = dist2_ref(q.x, q.y, q.z, p3.x, p3.y, p3.z);
-        pend[np * 32] = ((uint64_t)__float_as_uint(d0) << 32) | __float_as_uint(p0.w);
-        np += (__float_as_uint(d0) - wlo <= wspan) ? 1u : 0u;
-        pend[np * 32] = ((uint64_t)__float_as_uint(d1) << 32) | __float_as_uint(p1.w);
-        np += (__float_as_uint(d1) - wlo <= wspan) ? 1u : 0u;
-        pend[np * 32] = ((uint64_t)__float_as_uint(d2) << 32) | __float_as_uint(p2.w);
-        np += (__float_as_uint(d2) - wlo <= wspan) ? 1u : 0u;
-        pend[np * 32] = ((uint64_t)__float_as_uint(d3) << 32) | __float_as_uint(p3.w);
-        np += (__float_as_uint(d3) - wlo <= wspan) ? 1u : 0u;
+        test_pair(pk2(p0.x, p1.x), pk2(p0.y, p1.y), pk2(p0.z, p1.z), __float_as_uint(p0.w),
+                  __float_as_uint(p1.w));
+        test_pair(pk2(p2.x, p3.x), pk2(p2.y, p3.y), pk2(p2.z, p3.z), __float_as_uint(p2.w),
+                  __float_as_uint(p3.w));
       };
       auto check = [&]() {
         if (__any_sync(0xffffffffu, np > kPending - kCheck)) {
@@ -313,7 +369,7 @@ k_search(SearchArgs a) {
               keep = ex * ex + ey * ey + ez * ez <= R2k;
             }
             const uint32_t m = __ballot_sync(0xffffffffu, keep);
-            if (keep) stage[sc + __popc(m & lt)] = p;
+            if (keep) stage_put(stage, sc + __popc(m & lt), p);
             sc += __popc(m);
             loaded += min(32u, e0 - b);
             tested += __popc(m);
@@ -321,12 +377,15 @@ k_search(SearchArgs a) {
               __syncwarp();
 #pragma unroll 2
               for (int c0 = 0; c0 < 32; c0 += kCheck) {
-                test4(stage[c0], stage[c0 + 1], stage[c0 + 2], stage[c0 + 3]);
+                test4_staged(c0);
                 check();
               }
               __syncwarp();
               sc -= 32;
-              if (lane < sc) stage[lane] = stage[32 + lane];
+              float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
+              if (lane < sc) carry = stage_get(stage, 32 + lane);
+              __syncwarp();
+              if (lane < sc) stage_put(stage, lane, carry);
               __syncwarp();
             }
           }
@@ -334,10 +393,10 @@ k_search(SearchArgs a) {
       }
       if (sc > 0) {
         // pad the last batch with points at infinity: their distance never passes
-        if (lane >= sc) stage[lane] = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+        if (lane >= sc) stage_put(stage, lane, make_float4(INFINITY, INFINITY, INFINITY, 0.f));
         __syncwarp();
         for (uint32_t c0 = 0; c0 < sc; c0 += kCheck) {
-          test4(stage[c0], stage[c0 + 1], stage[c0 + 2], stage[c0 + 3]);
+          test4_staged((int)c0);
           check();
         }
         __syncwarp();
