@@ -160,6 +160,10 @@ typedef struct rtnn_tuning {
   float lane_walk_ratio;      /* a 32-query tile whose extent exceeds ratio x its search width
                                  is searched lane by lane (each lane walks its own query's
                                  cells) instead of sharing one candidate stream; 0: never */
+  float gap_ratio;            /* a tile is split into runs wherever two consecutive queries
+                                 (sort order) are farther apart than ratio x its widest search
+                                 width, so one candidate box never spans a jump of the Morton
+                                 curve; 0: split only between clouds */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

@@ -101,7 +101,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
@@ -386,6 +386,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.r2 = pr.radius * pr.radius;
   a.k = pr.k;
   a.lane_walk_ratio = tu.lane_walk_ratio;
+  a.gap_ratio = tu.gap_ratio;
   a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
             ((pr.flags & RTNN_FLAG_LOCAL_INDICES) ? kSearchLocalIndices : 0u);
   const int wpb = (int)std::max(1u, std::min(8u, tu.warps_per_block));
@@ -600,7 +601,7 @@ rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
       !(t->min_cell_ratio > 0.f && t->min_cell_ratio <= t->cell_ratio) ||
       !(t->points_per_cell >= 0.f) || t->fallback_passes > kMaxPasses - 2 ||
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f) ||
-      !(t->lane_walk_ratio >= 0.f))
+      !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
   return RTNN_OK;

@@ -37,6 +37,8 @@ struct SearchArgs {
   uint32_t flags;              // kSearch*
   int pass;                    // kPassMain, kPassEscalate or kPassFinal
   float lane_walk_ratio;       // tile spread > ratio * width: per-lane walk (0: never)
+  float gap_ratio;             // split a tile where consecutive queries are farther apart
+                               // than ratio * width (0: split at cloud changes only)
 };
 constexpr int kPassMain = 0;      // sorted queries, widths from the partition
 constexpr int kPassEscalate = 1;  // fallback list at its (doubled) widths

@@ -201,11 +201,29 @@ k_search(SearchArgs a) {
     valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
 
     bool short_lane = false;   // narrowed search that found fewer than K neighbors
+    // The tile is searched as runs of consecutive queries: a run ends where the next query
+    // (in sort order) belongs to another cloud or lies farther than gap_ratio x the widest
+    // width from its predecessor, so a jump of the Morton curve never stretches one
+    // candidate box over the space between two distant groups.
+    const float gap = a.gap_ratio * wmax(valid ? w : 0.f);
+    const float prx = __shfl_up_sync(0xffffffffu, q.x, 1);
+    const float pry = __shfl_up_sync(0xffffffffu, q.y, 1);
+    const float prz = __shfl_up_sync(0xffffffffu, q.z, 1);
+    const uint32_t prc = __shfl_up_sync(0xffffffffu, cloud, 1);
+    const bool prv = __shfl_up_sync(0xffffffffu, valid ? 1u : 0u, 1) != 0u;
+    bool run_start = valid && (lane == 0 || !prv || prc != cloud);
+    if (valid && !run_start && a.gap_ratio > 0.f) {
+      const float ex = q.x - prx, ey = q.y - pry, ez = q.z - prz;
+      run_start = ex * ex + ey * ey + ez * ez > gap * gap;
+    }
+    const uint32_t starts = __ballot_sync(0xffffffffu, run_start);
     uint32_t pending = __ballot_sync(0xffffffffu, valid);
     while (pending) {
-      const int leader = __ffs(pending) - 1;
+      const int leader = __ffs(pending) - 1;   // always a run start
+      const uint32_t later = starts & ~((2u << leader) - 1u);
+      const int next = later ? __ffs(later) - 1 : 32;
+      const uint32_t group = pending & (next == 32 ? 0xffffffffu : ((1u << next) - 1u));
       const uint32_t gcloud = __shfl_sync(0xffffffffu, cloud, leader);
-      const uint32_t group = __ballot_sync(0xffffffffu, valid && cloud == gcloud) & pending;
       pending &= ~group;
       const bool act = (group >> lane) & 1u;
 
