@@ -64,16 +64,23 @@ __device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-// dist2_ref of two points at once: ((dx*dx + dy*dy) + dz*dz), every step rounded
-__device__ __forceinline__ uint64_t dist2_pair(uint64_t qx, uint64_t qy, uint64_t qz, uint64_t px,
-                                               uint64_t py, uint64_t pz) {
+// dist2_ref of two points at once: ((dx*dx + dy*dy) + dz*dz), every step rounded.
+// Differences and squares are packed; the two sums are scalar __fadd_rn. A packed add
+// whose second operand is a packed product was measured to be fused into a single-rounding
+// multiply-add by the compiler even with .rn (about 12 % of results off by an ulp), which
+// would break the bit-exact distances; scalar adds after packed products matched scalar
+// arithmetic bit for bit on 2^20 random pairs.
+__device__ __forceinline__ void dist2_pair(uint64_t qx, uint64_t qy, uint64_t qz, uint64_t px,
+                                           uint64_t py, uint64_t pz, uint32_t& d0, uint32_t& d1) {
   const uint64_t dx = sub2(qx, px), dy = sub2(qy, py), dz = sub2(qz, pz);
-  return add2(add2(mul2(dx, dx), mul2(dy, dy)), mul2(dz, dz));
+  uint32_t x0, x1, y0, y1, z0, z1;
+  upk2(mul2(dx, dx), x0, x1);
+  upk2(mul2(dy, dy), y0, y1);
+  upk2(mul2(dz, dz), z0, z1);
+  d0 = __float_as_uint(__fadd_rn(__fadd_rn(__uint_as_float(x0), __uint_as_float(y0)),
+                                 __uint_as_float(z0)));
+  d1 = __float_as_uint(__fadd_rn(__fadd_rn(__uint_as_float(x1), __uint_as_float(y1)),
+                                 __uint_as_float(z1)));
 }
 
 // Staged candidates are kept in pairs, {x0 x1 y0 y1 | z0 z1 w0 w1} (32 bytes per two
@@ -273,7 +280,7 @@ k_search(SearchArgs a) {
       const uint64_t qx2 = pk2(q.x, q.x), qy2 = pk2(q.y, q.y), qz2 = pk2(q.z, q.z);
       auto test_pair = [&](uint64_t px, uint64_t py, uint64_t pz, uint32_t i0, uint32_t i1) {
         uint32_t d0, d1;
-        upk2(dist2_pair(qx2, qy2, qz2, px, py, pz), d0, d1);
+        dist2_pair(qx2, qy2, qz2, px, py, pz, d0, d1);
         pend[np * 32] = ((uint64_t)d0 << 32) | i0;
         np += (d0 - wlo <= wspan) ? 1u : 0u;
         pend[np * 32] = ((uint64_t)d1 << 32) | i1;
