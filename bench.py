@@ -261,6 +261,21 @@ def cpu_reference_sample(cfg, seconds, threads, seed=0):
                       f"{elapsed:.1f} s on {threads} host threads"}
 
 
+def reduce_max(x, dist=None, device="cpu"):
+    """Max over ranks of a per-rank scalar (the whole-job time is the slowest rank's)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(queries_per_rank, world, ms_max):
+    """Whole-job queries/s: every rank searched its own instance (weak scaling)."""
+    return world * queries_per_rank / (ms_max * 1e-3)
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -326,22 +341,30 @@ def run_rtnn(args, rank, world):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
+
+    # SPH workload: every step first moves each particle by N(0, 0.05 h), then rebuilds the
+    # grid and searches (the rebuild is part of every step anyway)
+    sph = cfg["name"] == "sph_lattice_5e7"
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    noise = torch.empty_like(tp) if sph else None
+
+    def step(plan):
+        if sph:
+            noise.normal_(0.0, 0.05, generator=gen)
+            tp.add_(noise)
+        plan.execute(tp, tq, out)
 
     def timed(plan, steps, warmup, clocks=None):
         for _ in range(warmup):
-            plan.execute(tp, tq, out)
+            step(plan)
         barrier()
         if clocks:
             clocks.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
-            plan.execute(tp, tq, out)
+            step(plan)
         e1.record(stream)
         barrier()
         ck = clocks.stop() if clocks else None
@@ -357,8 +380,6 @@ def run_rtnn(args, rank, world):
         plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, use_cache=False, **common)
         plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
         plain_ms, _ = timed(plain, args.steps, max(1, args.warmup // 2))
-        plain.execute(tp, tq, out)
-        result_plain = _row_sets(out)
         plain.close()
 
     # learned partition: grid knobs tuned on the analytic partition, the width model
@@ -375,8 +396,37 @@ def run_rtnn(args, rank, world):
     launches_per_step = st.n_launches
     fallback = st.n_fallback
     learned.close()
-    identical = None if result_plain is None else bool(torch.equal(_row_sets(out), result_plain))
-    del result_plain
+    identical = None
+    if not args.no_plain:   # same positions, plain vs learned: identical neighbor sets
+        result_learned = _row_sets(out)
+        check = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=False, **common)
+        check.execute(tp, tq, out)
+        check.close()
+        identical = bool(torch.equal(_row_sets(out), result_learned))
+        del result_learned
+
+    # batched vs a per-cloud launch loop (one rtnn_search per cloud, same flags/tuning)
+    loop_ms = None
+    n_clouds = int(len(cfg["offsets"]) - 1)
+    if n_clouds > 1:
+        off = cfg["offsets"]
+        qoff = cfg["qoffsets"]
+
+        def loop_once():
+            for c in range(n_clouds):
+                a, b = int(off[c]), int(off[c + 1])
+                qa, qb = (a, b) if qoff is None else (int(qoff[c]), int(qoff[c + 1]))
+                if b > a and qb > qa:
+                    ctx.search(tp[a:b], None if tq is None else tq[qa:qb], out=out[qa:qb],
+                               learned=True, **common)
+        loop_once()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        loop_once()
+        e1.record(stream)
+        barrier()
+        loop_ms = max_over_ranks(e0.elapsed_time(e1))
 
     # dominant kernel (search, both passes) timed with the library's events on `stream`
     nog = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=False, **common)
@@ -429,6 +479,8 @@ def run_rtnn(args, rank, world):
                        "n_clouds": int(len(cfg["offsets"]) - 1),
                        "path": "learned partition + batched persistent search, CUDA graph",
                        "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "per_cloud_loop_value": None if loop_ms is None else world * Q / (loop_ms * 1e-3),
+            "batched_over_loop": None if loop_ms is None else loop_ms / ms_learned,
             "plain_value": None if plain_ms is None else world * Q / (plain_ms * 1e-3),
             "learned_over_plain": None if plain_ms is None else plain_ms / ms_learned,
             "identical_sets": identical, "fallback_queries": int(fallback),
