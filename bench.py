@@ -34,6 +34,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+# DRAM bytes (read + write) per query of the main search pass, from the ncu capture in
+# profiles/k_search_knn_multicloud_scale0.1.md (866 MB for 5.25 M queries), scaled by
+# queries to a full launch; only known for the default workload.
+TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 165.0}
 
 
 def parse():
@@ -445,7 +449,10 @@ def run_rtnn(args, rank, world):
     achieved = alg_bytes / (ms_s * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
-                "traffic": None, "kernel": "k_search (both passes)", "peak_source": pk_src,
+                "traffic": (round(TRAFFIC_PER_QUERY[args.workload] * Q)
+                            if args.workload in TRAFFIC_PER_QUERY else None),
+                "traffic_scope": "main search pass, ncu at scale 0.1 scaled by queries",
+                "kernel": "k_search (all passes)", "peak_source": pk_src,
                 "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": round(ms_s, 4)}
 
     e2e = None
