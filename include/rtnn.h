@@ -169,6 +169,13 @@ typedef struct rtnn_tuning {
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);
 rtnn_status rtnn_set_tuning(rtnn_ctx* ctx, const rtnn_tuning* tuning);
 
+/* Failure-detection self-test (no counterpart in the reference, which has no device-side
+ * waits): runs the decoupled look-back scan with a predecessor tile that is never
+ * published, so its bounded wait (about a second) gives up. Returns
+ * RTNN_ERR_DEVICE_TIMEOUT when the limit works -- the expected result -- and leaves the
+ * context usable; any other status means the wait did not report. */
+rtnn_status rtnn_selftest_wait_timeout(rtnn_ctx* ctx);
+
 /* Search for callers that cannot allocate device memory. It has no counterpart in the
  * reference. For hosts that own all device memory through
  * their own pool, real-time loops that cannot afford cudaMalloc's implicit synchronisation,

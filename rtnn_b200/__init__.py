@@ -109,6 +109,7 @@ _SIGS = {
     "rtnn_mlp_adam_step": (_I, [_P, _P, _P, _P, _P, _F, _U32, _F]),
     "rtnn_search_noalloc": (_I, [_P, _U32, _P, _U32, _I, _F, _U32, _P, _P, ctypes.c_char_p,
                                  ctypes.c_size_t]),
+    "rtnn_selftest_wait_timeout": (_I, [_P]),
 }
 
 

@@ -857,6 +857,33 @@ rtnn_status rtnn_mlp_adam_step(rtnn_ctx* c, float* d_params, const float* d_grad
   return RTNN_OK;
 }
 
+rtnn_status rtnn_selftest_wait_timeout(rtnn_ctx* c) {
+  if (!c) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  // two scan tiles; the tile counter starts at 1, so the only working block takes tile 1
+  // and waits on tile 0, which no block ever publishes: the bounded look-back must give up
+  const uint64_t n = 2ull * kScanTile;
+  RTNN_CU(ensure(c->ws.cells, n * 4), "alloc");
+  RTNN_CU(ensure(c->ws.scan_state, scan_tiles_for(n) * 8), "alloc");
+  RTNN_CU(ensure(c->ws.counters, sizeof(Counters)), "alloc");
+  Counters* ctr = (Counters*)c->ws.counters.p;
+  static const uint32_t one = 1;
+  RTNN_CU(cudaMemsetAsync(c->ws.cells.p, 0, n * 4, s), "memset");
+  RTNN_CU(cudaMemsetAsync(ctr, 0, sizeof(Counters), s), "memset");
+  RTNN_CU(cudaMemcpyAsync(&ctr->scan_tiles[0], &one, 4, cudaMemcpyHostToDevice, s), "copy");
+  RTNN_CU(launch_scan_excl((uint32_t*)c->ws.cells.p, n, nullptr, 0, n,
+                           (uint64_t*)c->ws.scan_state.p, &ctr->scan_tiles[0], ctr, s),
+          "scan");
+  RTNN_CU(cudaMemcpyAsync(c->h_ctr, ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "copy");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  if (c->h_ctr->error == kErrScanTimeout)
+    return fail(c, RTNN_ERR_DEVICE_TIMEOUT, "scan look-back gave up waiting on tile " +
+                                                std::to_string(c->h_ctr->error_info));
+  return fail(c, RTNN_ERR_INTERNAL, "the bounded wait did not report a timeout");
+}
+
 rtnn_status rtnn_model_train(rtnn_ctx* c, const float* d_feats, const float* d_target,
                              uint64_t n, uint32_t epochs, uint32_t batch, float lr,
                              uint64_t seed, float* loss_per_epoch) {

@@ -286,3 +286,19 @@ def test_walk_modes_give_identical_rows(ctx, ratio):
             assert np.array_equal(got, oracle.grid_search(u, None, mode, 3.0, 40))
     finally:
         ctx.set_tuning(**base)
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(ctx):
+    """A device-side wait that can never be satisfied (a scan predecessor nobody
+    publishes) gives up after its limit and reports RTNN_ERR_DEVICE_TIMEOUT; the context
+    and the GPU stay usable."""
+    import time
+    lib = rtnn_b200.load_library()
+    t0 = time.time()
+    st = lib.rtnn_selftest_wait_timeout(ctx.handle)
+    assert st == 5, lib.rtnn_last_error(ctx.handle)   # RTNN_ERR_DEVICE_TIMEOUT
+    assert time.time() - t0 < 60
+    assert b"gave up" in lib.rtnn_last_error(ctx.handle)
+    p = wl.uniform_cube(5000, 20.0, seed=1)
+    got = ctx.search(p, None, "radius", 2.0, 16, sorted_rows=True)
+    assert np.array_equal(got, oracle.grid_search(p, None, "radius", 2.0, 16))
