@@ -61,6 +61,9 @@ typedef enum rtnn_mode {
                                            fallback (replaces the analytic heuristic) */
 #define RTNN_FLAG_SORTED_ROWS     0x8u  /* sort each output row by (distance, index) */
 #define RTNN_FLAG_LOCAL_INDICES   0x10u /* batched: indices relative to the point's own cloud */
+#define RTNN_FLAG_ANY_K           0x20u /* any K of the qualifying points (the first found),
+                                           not the K nearest: the reference's radius-search
+                                           semantics (geometry.cu:72-83), cheaper */
 
 /* Per-call statistics (all optional to read). Times are device times measured with
  * CUDA events on the context stream (graph replays report ms_total only). */

@@ -24,6 +24,7 @@ FLAG_PARTITION = 0x2
 FLAG_LEARNED = 0x4
 FLAG_SORTED_ROWS = 0x8
 FLAG_LOCAL_INDICES = 0x10
+FLAG_ANY_K = 0x20
 MAX_K = 128
 
 _STATUS = {
@@ -196,17 +197,19 @@ class Context:
 
     # -- single cloud -------------------------------------------------------------------
     def search(self, points, queries=None, mode="radius", radius=2.0, k=50, partition=False,
-               learned=False, sorted_rows=False, out=None, stats=None):
+               learned=False, sorted_rows=False, any_k=False, out=None, stats=None):
         """Neighbors of every query: [Q, k] int32, -1 in unused slots.
 
         points / queries: numpy [n, 3] float32 (host; copies happen inside the call) or
         CUDA torch tensors [n, 3] float32 (device; `out` may be a preallocated CUDA
         int32 tensor [Q, k]). mode: "radius" (self included) or "knn" (0 < d < r^2).
+        any_k: any K qualifying points (the reference's radius semantics) instead of the
+        K nearest.
         """
         lib = load_library()
         m = _mode(mode)
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
-                 (FLAG_SORTED_ROWS if sorted_rows else 0))
+                 (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_ANY_K if any_k else 0))
         st = stats if stats is not None else Stats()
         if _is_torch(points):
             import torch

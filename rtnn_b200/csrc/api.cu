@@ -151,7 +151,7 @@ rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32
   if (N >= (1ull << 31) || Q >= (1ull << 31))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 points and queries");
   const uint32_t known = RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED |
-                         RTNN_FLAG_SORTED_ROWS | RTNN_FLAG_LOCAL_INDICES;
+                         RTNN_FLAG_SORTED_ROWS | RTNN_FLAG_LOCAL_INDICES | RTNN_FLAG_ANY_K;
   if (flags & ~known) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "unknown flag bits");
   if ((flags & RTNN_FLAG_LEARNED) && !c->has_model)
     return fail(c, RTNN_ERR_NO_MODEL, "RTNN_FLAG_LEARNED needs a width model (rtnn_model_set or rtnn_model_train)");
@@ -388,7 +388,8 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.lane_walk_ratio = tu.lane_walk_ratio;
   a.gap_ratio = tu.gap_ratio;
   a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
-            ((pr.flags & RTNN_FLAG_LOCAL_INDICES) ? kSearchLocalIndices : 0u);
+            ((pr.flags & RTNN_FLAG_LOCAL_INDICES) ? kSearchLocalIndices : 0u) |
+            ((pr.flags & RTNN_FLAG_ANY_K) ? kSearchAnyK : 0u);
   const int wpb = (int)std::max(1u, std::min(8u, tu.warps_per_block));
   int bps = search_blocks_per_sm(knn, pr.k, wpb);
   if (tu.blocks_per_sm > 0) bps = std::min(bps, (int)tu.blocks_per_sm);

@@ -9,6 +9,7 @@ namespace rtnn {
 
 constexpr uint32_t kSearchSortedRows = 1u;
 constexpr uint32_t kSearchLocalIndices = 2u;
+constexpr uint32_t kSearchAnyK = 4u;          // stop at the first K qualifying points
 
 struct SearchArgs {
   CloudTables t;

@@ -121,9 +121,10 @@ __device__ __forceinline__ void hit_window(bool active, float lim, float root_d,
 // heapified (max-heap on (distance, index)) and later hits replace the root when smaller.
 // Kept out of line: it is reached from several places of the test loop, and one copy keeps
 // the search kernel's hot loop small enough for the instruction cache.
+// With any_k the first k hits are kept as they come and later ones are dropped.
 __device__ __noinline__ void flush_pending(uint64_t* heap, const uint64_t* pend, uint32_t& np,
                                            uint32_t& n, uint32_t k, uint64_t& root,
-                                           float& root_d) {
+                                           float& root_d, bool any_k) {
   const uint32_t steps = __reduce_max_sync(0xffffffffu, np);
   for (uint32_t i = 0; i < steps; ++i) {
     if (i < np) {
@@ -131,12 +132,12 @@ __device__ __noinline__ void flush_pending(uint64_t* heap, const uint64_t* pend,
       if (n < k) {
         heap[n * 32] = key;
         ++n;
-        if (n == k) {
+        if (n == k && !any_k) {
           for (int j = (int)k / 2 - 1; j >= 0; --j) heap_sift_down(heap, j, k, heap[j * 32]);
           root = heap[0];
           root_d = __uint_as_float((uint32_t)(root >> 32));
         }
-      } else if (key < root) {
+      } else if (!any_k && key < root) {
         heap_sift_down(heap, 0, k, key);
         root = heap[0];
         root_d = __uint_as_float((uint32_t)(root >> 32));
@@ -171,6 +172,7 @@ k_search(SearchArgs a) {
   const uint32_t k = a.k;
   const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
   const bool local_idx = (a.flags & kSearchLocalIndices) != 0;
+  const bool any_k = (a.flags & kSearchAnyK) != 0;
   const bool main_pass = a.pass == kPassMain;
   const uint32_t fb_total = main_pass ? 0u : *a.fb_in_count;
   const uint32_t n_tiles = main_pass ? a.n_tiles : (fb_total + 31) / 32;
@@ -270,7 +272,7 @@ k_search(SearchArgs a) {
       uint32_t loaded = 0, tested = 0;   // work counters of this group (warp-uniform)
       // hit test on the distance bits: lo <= bits(d) <= lo + span (see hit_window)
       uint32_t wlo, wspan;
-      hit_window(act, lim_l, root_d, KNN, wlo, wspan);
+      hit_window(act && !(any_k && n >= k), lim_l, root_d, KNN, wlo, wspan);
 
       // 4. every lane against a staged point; a hit only appends to the lane's pending
       //    buffer, and the heaps are updated by the whole warp at once once some lane
@@ -305,8 +307,8 @@ k_search(SearchArgs a) {
       };
       auto check = [&]() {
         if (__any_sync(0xffffffffu, np > kPending - kCheck)) {
-          flush_pending(heap, pend, np, n, k, root, root_d);
-          hit_window(act, lim_l, root_d, KNN, wlo, wspan);
+          flush_pending(heap, pend, np, n, k, root, root_d, any_k);
+          hit_window(act && !(any_k && n >= k), lim_l, root_d, KNN, wlo, wspan);
         }
       };
       uint32_t sc = 0;   // staged candidates (warp-uniform, < 32 between batches)
@@ -427,7 +429,7 @@ k_search(SearchArgs a) {
         __syncwarp();
       }
 
-      flush_pending(heap, pend, np, n, k, root, root_d);
+      flush_pending(heap, pend, np, n, k, root, root_d, any_k);
       if (lane == 0 && loaded) {
         atomicAdd(&a.ctr->n_loaded, (unsigned long long)loaded);
         atomicAdd(&a.ctr->n_tested, (unsigned long long)tested);

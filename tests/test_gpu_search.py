@@ -302,3 +302,19 @@ def test_bounded_wait_reports_timeout_and_context_survives(ctx):
     p = wl.uniform_cube(5000, 20.0, seed=1)
     got = ctx.search(p, None, "radius", 2.0, 16, sorted_rows=True)
     assert np.array_equal(got, oracle.grid_search(p, None, "radius", 2.0, 16))
+
+
+@pytest.mark.parametrize("mode", ["radius", "knn"])
+def test_any_k_returns_k_qualifying_points(ctx, mode):
+    """RTNN_FLAG_ANY_K: every row holds min(K, #qualifying) distinct qualifying points
+    (the reference's radius semantics); which ones is unspecified."""
+    p = wl.uniform_cube(30_000, 30.0, seed=6)
+    k, r = 12, 2.5
+    full = oracle.grid_search(p, None, mode, r, 128)
+    got = ctx.search(p, None, mode, r, k, any_k=True)
+    n_q = (full >= 0).sum(1)
+    assert np.array_equal((got >= 0).sum(1), np.minimum(n_q, k))
+    for qi in range(0, p.shape[0], 97):
+        g = got[qi][got[qi] >= 0]
+        assert len(set(g.tolist())) == len(g)
+        assert set(g.tolist()) <= set(full[qi][full[qi] >= 0].tolist())
