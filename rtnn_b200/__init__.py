@@ -239,14 +239,15 @@ class Context:
     # -- many clouds --------------------------------------------------------------------
     def search_batched(self, points, point_offsets, queries=None, query_offsets=None,
                        mode="knn", radius=0.2, k=32, partition=False, learned=False,
-                       sorted_rows=False, local_indices=False, out=None, stats=None):
+                       sorted_rows=False, local_indices=False, any_k=False, out=None, stats=None):
         """Many independent clouds in one launch; offsets have n_clouds + 1 entries."""
         lib = load_library()
         po = np.ascontiguousarray(np.asarray(point_offsets, dtype=np.uint64))
         qo = None if query_offsets is None else np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64))
         n_clouds = po.shape[0] - 1
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
-                 (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0))
+                 (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0) |
+                 (FLAG_ANY_K if any_k else 0))
         st = stats if stats is not None else Stats()
         nq = int(po[-1]) if queries is None else int(qo[-1])
         if _is_torch(points):
@@ -272,9 +273,9 @@ class Context:
 
     def plan(self, point_offsets, query_offsets=None, mode="knn", radius=0.2, k=32,
              partition=False, learned=False, sorted_rows=False, local_indices=False,
-             use_graph=True):
+             use_graph=True, any_k=False):
         return Plan(self, point_offsets, query_offsets, mode, radius, k, partition, learned,
-                    sorted_rows, local_indices, use_graph)
+                    sorted_rows, local_indices, use_graph, any_k)
 
     # -- learned widths -------------------------------------------------------------------
     def model_size(self):
@@ -347,13 +348,14 @@ class Plan:
     """Fixed-shape batched search replayed from a CUDA graph (rtnn_plan_*)."""
 
     def __init__(self, ctx, point_offsets, query_offsets, mode, radius, k, partition, learned,
-                 sorted_rows, local_indices, use_graph):
+                 sorted_rows, local_indices, use_graph, any_k=False):
         self.ctx = ctx
         lib = load_library()
         po = np.ascontiguousarray(np.asarray(point_offsets, dtype=np.uint64))
         qo = None if query_offsets is None else np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64))
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
-                 (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0))
+                 (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0) |
+                 (FLAG_ANY_K if any_k else 0))
         self.k = k
         self.n_queries = int((qo if qo is not None else po)[-1])
         h = _P()
