@@ -6,6 +6,7 @@ only as the checker or the timed CPU reference; the library (rtnn_b200) never im
 - liboracle.so (oracle.c): FP32 restatement of the reference's distance and predicates,
   brute force and grid-accelerated, plus an FP64 brute force and the FP32/FP64 boundary
   pairs.
+  Also the reference's point-cloud text reader (util.cpp:100-135), for the CLI's.
 - _ref/refcheck: the reference's own check.cpp (sanityCheckRadius / sanityCheckKNN),
   compiled from the reference sources by oracle/Makefile.
 - _ref/libref.so: the reference's calcSearchSize / MortonCode3 (grid.cu,
@@ -57,6 +58,8 @@ def lib():
         L.oracle_ref_shell_mask.argtypes = [_P] + [ctypes.c_int] * 6 + [ctypes.c_float,
                                                                          ctypes.c_float,
                                                                          ctypes.c_uint32]
+        L.oracle_read_pc.restype = ctypes.c_int64
+        L.oracle_read_pc.argtypes = [ctypes.c_char_p, _P, _U64]
         L.oracle_box_counts.restype = None
         L.oracle_box_counts.argtypes = [_P] + [ctypes.c_int] * 7 + [_P]
         _lib = L
@@ -123,6 +126,17 @@ def boundary_pairs(points, queries=None, mode="radius", r=2.0, max_pairs=100000)
                                     q.shape[0], _mode(mode), float(r), buf.ctypes.data_as(_P),
                                     max_pairs)
     return buf[:min(n, max_pairs)].copy()
+
+
+def read_pc(path):
+    """Points of a text file as the reference's reader gives them: [n, 3] float32."""
+    L = lib()
+    n = L.oracle_read_pc(os.fsencode(path), None, 0)
+    if n < 0:
+        raise FileNotFoundError(path)
+    out = np.zeros((n, 3), dtype=np.float32)
+    L.oracle_read_pc(os.fsencode(path), out.ctypes.data_as(_P), n)
+    return out
 
 
 def box_counts(counts, cx, cy, cz, shells=3):

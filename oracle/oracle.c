@@ -23,6 +23,7 @@
  * oracle/Makefile into oracle/_ref/refcheck) and against the FP64 brute force below.
  */
 #include <math.h>
+#include <stdio.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -358,4 +359,41 @@ int oracle_ref_shell_mask(const uint32_t* counts, int dx, int dy, int dz, int cx
              CNT(x1, y0, z0) + CNT(x1, y0, z1) + CNT(x1, y1, z0) + CNT(x1, y1, z1);
   }
 #undef CNT
+}
+
+/* Point-cloud text reader as the reference's read_pc_data (src/optixNSearch/util.cpp:
+ * 100-135): lines are read into a 1024-byte buffer (std::istream::getline: at most 1023
+ * characters; a longer line, or a line of 1023 characters not followed by its '\n',
+ * ends the read, and a last line without '\n' still counts), and each line goes through
+ * sscanf("%lf,%lf,%lf\n") with the doubles cast to float. A field sscanf does not assign
+ * is 0 here (the reference leaves it unset). Writes up to `cap` points into xyz and
+ * returns the number of points in the file, or -1 when it cannot be opened. */
+int64_t oracle_read_pc(const char* path, float* xyz, uint64_t cap) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return -1;
+  char line[1024];
+  int64_t n = 0;
+  for (;;) {
+    size_t len = 0;
+    int c, got_delim = 0, any = 0;
+    while ((c = fgetc(f)) != EOF) {
+      any = 1;
+      if (c == '\n') { got_delim = 1; break; }
+      if (len == 1023) { len = 1024; break; }  /* getline: n-1 stored, no delimiter */
+      line[len++] = (char)c;
+    }
+    if (len == 1024 || !any) break;          /* failbit: the read ends */
+    (void)got_delim;
+    line[len] = '\0';
+    double x = 0, y = 0, z = 0;
+    sscanf(line, "%lf,%lf,%lf\n", &x, &y, &z);
+    if ((uint64_t)n < cap) {
+      xyz[3 * n + 0] = (float)x;
+      xyz[3 * n + 1] = (float)y;
+      xyz[3 * n + 2] = (float)z;
+    }
+    ++n;
+  }
+  fclose(f);
+  return n;
 }

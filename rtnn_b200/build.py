@@ -70,10 +70,10 @@ def build(verbose=False, ptxas_verbose=False):
     if _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs +
              ["-Xlinker", "--no-undefined", "-Xlinker", "-z,defs"], verbose)
-    cli_src = os.path.join(CSRC, "cli.cpp")
-    if os.path.exists(cli_src) and _stale(CLI, [cli_src, LIB] + hdrs):
-        _run(["g++", "-O2", "-std=c++17", "-I" + INCLUDE, cli_src, "-o", CLI, "-L" + LIBDIR,
-              "-lrtnn_b200", "-Wl,-rpath,$ORIGIN/../lib"], verbose)
+    cli_srcs = [os.path.join(CSRC, f) for f in ("cli.cpp", "pointio.cpp")]
+    if _stale(CLI, cli_srcs + [LIB, os.path.join(CSRC, "pointio.h")] + hdrs):
+        _run(["g++", "-O2", "-std=c++17", "-pthread", "-I" + INCLUDE] + cli_srcs +
+             ["-o", CLI, "-L" + LIBDIR, "-lrtnn_b200", "-Wl,-rpath,$ORIGIN/../lib"], verbose)
     return LIB
 
 

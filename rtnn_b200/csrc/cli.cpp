@@ -8,8 +8,12 @@
 // the KNN K is fixed when the binary is built (RTNN_KNN, default 5) and -k only applies to
 // radius search (util.cpp:367-369). Input files hold one "x,y,z" point per line, read as
 // double and cast to float (util.cpp:101-135).
+// Points files ending in .bin or .f32 hold raw float32 x,y,z triples; text files are parsed
+// on all host threads (pointio.cpp).
 // Extra flags: -o FILE (write the int32 result rows), -lm FILE (learned width model,
-// raw float32), --parse-only (print the parsed points' count and checksum and exit).
+// raw float32), --parse-only (print the parsed points' count and checksum and exit),
+// --convert FILE (write the parsed points as raw float32 and exit), --threads N (text
+// parser threads, 0 = all).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -22,6 +26,7 @@
 #include <string>
 #include <vector>
 
+#include "pointio.h"
 #include "rtnn.h"
 #include "rtnn_learn.h"
 
@@ -32,7 +37,8 @@
 namespace {
 
 struct Options {
-  std::string pfile, qfile, search_mode = "radius", out_file, model_file;
+  std::string pfile, qfile, search_mode = "radius", out_file, model_file, convert_file;
+  unsigned threads = 0;
   float radius = 2.0f;
   unsigned knn = 50;
   int device = 0;
@@ -51,7 +57,9 @@ void usage(const char* argv0) {
                "  --check      | -c   Sanity check the result (default 0).\n"
                "  --partition  | -p   Density-bucket partitioning (default 1).\n"
                "  -o FILE  write the result rows (int32, -1 = none); -lm FILE learned model;\n"
-               "  --parse-only  print the parsed points and exit.\n",
+               "  --parse-only  print the parsed points and exit; --convert FILE write them as\n"
+               "  raw float32 (*.f32 / *.bin, read back by -f/-q) and exit; --threads N parser\n"
+               "  threads (0 = all).\n",
                argv0, RTNN_KNN);
   std::exit(0);
 }
@@ -84,6 +92,8 @@ Options parse(int argc, char** argv) {
     else if (a == "-o") o.out_file = next();
     else if (a == "-lm") o.model_file = next();
     else if (a == "--parse-only") o.parse_only = true;
+    else if (a == "--convert") o.convert_file = next();
+    else if (a == "--threads") o.threads = (unsigned)std::atoi(next().c_str());
     else if (ignored.count(a)) {
       const std::string v = next();
       std::fprintf(stderr, "warning: %s %s has no effect in this build\n", a.c_str(), v.c_str());
@@ -97,21 +107,12 @@ Options parse(int argc, char** argv) {
   return o;
 }
 
-// One "x,y,z" per line, parsed as double then cast to float (util.cpp:101-135).
-std::vector<float> read_points(const std::string& path) {
-  std::ifstream f(path);
-  if (!f.good()) {
-    std::fprintf(stderr, "Could not read the frame data (%s)\n", path.c_str());
-    std::exit(1);
-  }
+std::vector<float> read_points(const std::string& path, unsigned threads) {
   std::vector<float> xyz;
-  std::string line;
-  while (std::getline(f, line)) {
-    double x = 0, y = 0, z = 0;
-    std::sscanf(line.c_str(), "%lf,%lf,%lf", &x, &y, &z);
-    xyz.push_back((float)x);
-    xyz.push_back((float)y);
-    xyz.push_back((float)z);
+  std::string err;
+  if (!rtnn::read_points_file(path, threads, &xyz, &err)) {
+    std::fprintf(stderr, "Could not read the frame data (%s)\n", err.c_str());
+    std::exit(1);
   }
   return xyz;
 }
@@ -168,11 +169,20 @@ bool sanity_check(const Options& o, const std::vector<float>& P, const std::vect
 
 int main(int argc, char** argv) {
   const Options o = parse(argc, argv);
-  std::vector<float> P = read_points(o.pfile);
+  std::vector<float> P = read_points(o.pfile, o.threads);
   const bool same = o.qfile.empty() || o.qfile == o.pfile;
-  std::vector<float> Qv = same ? std::vector<float>() : read_points(o.qfile);
+  std::vector<float> Qv = same ? std::vector<float>() : read_points(o.qfile, o.threads);
   const std::vector<float>& Q = same ? P : Qv;
   const uint64_t np = P.size() / 3, nq = Q.size() / 3;
+  if (!o.convert_file.empty()) {
+    std::string err;
+    if (!rtnn::write_points_f32(o.convert_file, P, &err)) {
+      std::fprintf(stderr, "%s\n", err.c_str());
+      return 1;
+    }
+    std::printf("points %llu written to %s\n", (unsigned long long)np, o.convert_file.c_str());
+    return 0;
+  }
   if (o.parse_only) {
     double sum = 0;
     for (float v : P) sum += v;
