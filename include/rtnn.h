@@ -167,6 +167,10 @@ typedef struct rtnn_tuning {
                                  (sort order) are farther apart than ratio x its widest search
                                  width, so one candidate box never spans a jump of the Morton
                                  curve; 0: split only between clouds */
+  uint32_t pending_slots;     /* per query, shared-memory slots for hits found since the last
+                                 merge into its K kept neighbors (8..256); more slots mean
+                                 fewer merges and fewer resident warps. Reduced when K +
+                                 slots would not fit one warp's shared memory */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

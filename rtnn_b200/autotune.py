@@ -24,6 +24,7 @@ GRID_KNOBS = [
     ("warps_per_block", [2, 4]),
     ("lane_walk_ratio", [0.0, 0.5, 1.0, 2.0]),
     ("gap_ratio", [0.0, 1.0, 2.0, 4.0]),
+    ("pending_slots", [8, 16, 32, 64]),
 ]
 LEARNED_KNOBS = [
     ("width_margin", [1.15, 1.3, 1.6]),

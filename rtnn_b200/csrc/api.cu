@@ -101,7 +101,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f, 16u};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
@@ -390,8 +390,9 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
             ((pr.flags & RTNN_FLAG_LOCAL_INDICES) ? kSearchLocalIndices : 0u) |
             ((pr.flags & RTNN_FLAG_ANY_K) ? kSearchAnyK : 0u);
-  const int wpb = (int)std::max(1u, std::min(8u, tu.warps_per_block));
-  int bps = search_blocks_per_sm(knn, pr.k, wpb);
+  int wpb = 4;
+  fit_search_shape(pr.k, tu.pending_slots, (int)tu.warps_per_block, &a.pending, &wpb);
+  int bps = search_blocks_per_sm(knn, pr.k, a.pending, wpb);
   if (tu.blocks_per_sm > 0) bps = std::min(bps, (int)tu.blocks_per_sm);
   const uint64_t persistent = (uint64_t)c->n_sms * bps;
   const uint64_t need_blocks = (sh.n_tiles + wpb - 1) / wpb;
@@ -602,7 +603,8 @@ rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
       !(t->min_cell_ratio > 0.f && t->min_cell_ratio <= t->cell_ratio) ||
       !(t->points_per_cell >= 0.f) || t->fallback_passes > kMaxPasses - 2 ||
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f) ||
-      !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f))
+      !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f) || t->pending_slots < 8 ||
+      t->pending_slots > 256)
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
   return RTNN_OK;

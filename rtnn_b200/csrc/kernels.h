@@ -35,6 +35,7 @@ struct SearchArgs {
   float radius;                // user radius r
   float r2;                    // fl(r * r)
   uint32_t k;
+  uint32_t pending;            // appended-hit slots per lane beyond the k kept ones
   uint32_t flags;              // kSearch*
   int pass;                    // kPassMain, kPassEscalate or kPassFinal
   float lane_walk_ratio;       // tile spread > ratio * width: per-lane walk (0: never)
@@ -84,9 +85,12 @@ cudaError_t launch_gather_queries(const float* xyz, const uint32_t* order, uint3
                                   cudaStream_t s);
 
 // search.cu
-size_t search_smem_bytes(uint32_t k, int warps_per_block);
+constexpr size_t kSearchSmemLimit = 227 * 1024;   // dynamic shared memory per block
+size_t search_smem_bytes(uint32_t k, uint32_t pending, int warps_per_block);
 cudaError_t search_prepare(int device);
-int search_blocks_per_sm(bool knn, uint32_t k, int warps_per_block);
+int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block);
+// appended-hit slots (multiple of 4, 8..256) and warps per block that fit the limit
+void fit_search_shape(uint32_t k, uint32_t pending_req, int wpb_req, uint32_t* pending, int* wpb);
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
                           cudaStream_t s);
 cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, const uint32_t* n_dev,

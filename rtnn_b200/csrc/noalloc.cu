@@ -184,8 +184,9 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
     a.r2 = radius * radius;
     a.k = k;
     a.pass = kPassMain;
-    const int wpb = 4;
-    const uint64_t blocks = (uint64_t)n_sms * search_blocks_per_sm(knn, k, wpb);
+    int wpb = 4;
+    fit_search_shape(k, 16u, 4, &a.pending, &wpb);
+    const uint64_t blocks = (uint64_t)n_sms * search_blocks_per_sm(knn, k, a.pending, wpb);
     const uint64_t need = (n_tiles + wpb - 1) / wpb;
     e = launch_search(knn, a, (unsigned)(blocks < need ? blocks : need), wpb, s);
   }

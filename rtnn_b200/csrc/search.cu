@@ -16,7 +16,8 @@
 //      __ballot_sync into a per-warp shared-memory stage;
 //   4. every lane tests every staged point against its own query with the reference's
 //      FP32 distance (common.cuh: dist2_ref) and keeps its K smallest (distance, index)
-//      pairs in a max-heap in shared memory ([slot][lane], conflict-free columns);
+//      pairs in a per-lane column in shared memory ([slot][lane], conflict-free): hits are
+//      appended branch-free and merged into a max-heap of the K kept when a column fills;
 //   5. rows are written warp-cooperatively (coalesced), unused slots = -1.
 // Queries whose search width was narrowed by the partition (width < r) and that found
 // fewer than K neighbors inside it are appended to a fallback list; a second pass of
@@ -94,7 +95,6 @@ __device__ __forceinline__ float4 stage_get(const float* st, uint32_t slot) {
   return make_float4(b[0], b[2], b[4], b[6]);
 }
 
-constexpr uint32_t kPending = 8;   // per-lane hit buffer between heap updates
 constexpr int kCheck = 4;          // candidates tested between two buffer-full votes
 constexpr int kStage = 64;         // staged candidates per warp (float4)
 
@@ -116,35 +116,56 @@ __device__ __forceinline__ void hit_window(bool active, float lim, float root_d,
   }
 }
 
-// Moves every lane's pending hits into its heap (all lanes together, one hit each per
-// step). While the heap holds fewer than k entries hits are appended; at k it is
-// heapified (max-heap on (distance, index)) and later hits replace the root when smaller.
-// Kept out of line: it is reached from several places of the test loop, and one copy keeps
-// the search kernel's hot loop small enough for the instruction cache.
-// With any_k the first k hits are kept as they come and later ones are dropped.
-__device__ __noinline__ void flush_pending(uint64_t* heap, const uint64_t* pend, uint32_t& np,
-                                           uint32_t& n, uint32_t k, uint64_t& root,
-                                           float& root_d, bool any_k) {
-  const uint32_t steps = __reduce_max_sync(0xffffffffu, np);
-  for (uint32_t i = 0; i < steps; ++i) {
-    if (i < np) {
-      const uint64_t key = pend[i * 32];
-      if (n < k) {
-        heap[n * 32] = key;
-        ++n;
-        if (n == k && !any_k) {
-          for (int j = (int)k / 2 - 1; j >= 0; --j) heap_sift_down(heap, j, k, heap[j * 32]);
-          root = heap[0];
-          root_d = __uint_as_float((uint32_t)(root >> 32));
-        }
-      } else if (!any_k && key < root) {
-        heap_sift_down(heap, 0, k, key);
-        root = heap[0];
-        root_d = __uint_as_float((uint32_t)(root >> 32));
-      }
+// Per-lane result column in shared memory ([slot][lane], so lanes never share a bank):
+// slots [0, n) hold the lane's kept neighbors -- a max-heap on (distance, index) once
+// n == k -- and slots [n, fill) the hits appended since the last merge. The test loop
+// writes every candidate's key at slot `fill` and advances fill only on a hit, so an
+// append costs no branch; merge_column folds the appended hits in when some lane's
+// column is nearly full, and once at the end of a group. While fewer than k are kept
+// nothing moves (the hits are already in place); the merge that crosses k heapifies the
+// first k, and later hits replace the root when smaller.
+struct LaneTop {
+  uint64_t root;   // largest kept key once n == k (~0 before)
+  uint32_t n;      // kept entries
+  uint32_t fill;   // kept + appended entries
+};
+
+// Folds slots [n, fill) into the kept set. With any_k the first k hits are kept as they
+// came and later ones dropped. Out of line: it is reached from several places of the
+// test loop, and one copy keeps the hot loop small enough for the instruction cache.
+__device__ __noinline__ LaneTop merge_column(uint64_t* col, LaneTop s, uint32_t k, bool any_k) {
+  if (s.n < k) {
+    if (s.fill < k || any_k) {   // at exactly k the heap is built below
+      s.n = min(s.fill, k);
+      s.fill = s.n;
+      return s;
     }
+    for (int i = (int)k / 2 - 1; i >= 0; --i) heap_sift_down(col, (uint32_t)i, k, col[i * 32]);
+    s.root = col[0];
+    s.n = k;
   }
-  np = 0;
+  if (any_k) {
+    s.fill = k;
+    return s;
+  }
+  // slots >= k are never written by a sift, so the next key can be read ahead
+  uint64_t root = s.root;
+  uint64_t key = k < s.fill ? col[k * 32] : 0ull;
+  for (uint32_t j = k; j < s.fill; ++j) {
+    const uint64_t next = j + 1 < s.fill ? col[(j + 1) * 32] : 0ull;
+    if (key < root) {
+      heap_sift_down(col, 0, k, key);
+      root = col[0];
+    }
+    key = next;
+  }
+  s.root = root;
+  s.fill = k;
+  return s;
+}
+
+__device__ __forceinline__ float root_dist(const LaneTop& s, uint32_t k) {
+  return s.n == k ? __uint_as_float((uint32_t)(s.root >> 32)) : INFINITY;
 }
 
 __device__ __forceinline__ float wmin(float v) {
@@ -164,10 +185,10 @@ k_search(SearchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   float* stage = reinterpret_cast<float*>(smem) + warp * kStage * 4;   // pair layout
+  const uint32_t slots = a.k + a.pending;   // result column length per lane
   uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * kStage * 16) +
-                    (size_t)warp * (a.k + kPending) * 32;
-  uint64_t* heap = heapw + lane;   // this lane's column: heap[i * 32]
-  uint64_t* pend = heapw + (size_t)a.k * 32 + lane;   // pending hits: pend[i * 32]
+                    (size_t)warp * slots * 32;
+  uint64_t* col = heapw + lane;   // this lane's column: col[i * 32]
   const uint32_t lt = lanemask_lt();
   const uint32_t k = a.k;
   const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
@@ -265,28 +286,26 @@ k_search(SearchArgs a) {
       const int nrows = empty ? 0 : ny * nz;
 
       const float lim_l = act ? lim : -1.f;
-      uint32_t n = 0;
-      uint64_t root = ~0ull;
-      float root_d = INFINITY;
-      uint32_t np = 0;                   // pending hits of this lane
+      LaneTop top{~0ull, 0u, 0u};
+      uint32_t fill = 0;                 // kept + appended entries of this lane's column
       uint32_t loaded = 0, tested = 0;   // work counters of this group (warp-uniform)
       // hit test on the distance bits: lo <= bits(d) <= lo + span (see hit_window)
       uint32_t wlo, wspan;
-      hit_window(act && !(any_k && n >= k), lim_l, root_d, KNN, wlo, wspan);
+      hit_window(act, lim_l, INFINITY, KNN, wlo, wspan);
 
       // 4. every lane against a staged point; a hit only appends to the lane's pending
-      //    buffer, and the heaps are updated by the whole warp at once once some lane
-      //    holds more than kPending - kCheck hits (checked every kCheck candidates)
+      //    column, and the columns are merged once some lane's column has fewer than
+      //    kCheck free slots (checked every kCheck candidates)
       // four candidates at a time: loads first, four independent distance chains, then
       // branch-free appends (the slot is always written, the count moves on a hit only)
       const uint64_t qx2 = pk2(q.x, q.x), qy2 = pk2(q.y, q.y), qz2 = pk2(q.z, q.z);
       auto test_pair = [&](uint64_t px, uint64_t py, uint64_t pz, uint32_t i0, uint32_t i1) {
         uint32_t d0, d1;
         dist2_pair(qx2, qy2, qz2, px, py, pz, d0, d1);
-        pend[np * 32] = ((uint64_t)d0 << 32) | i0;
-        np += (d0 - wlo <= wspan) ? 1u : 0u;
-        pend[np * 32] = ((uint64_t)d1 << 32) | i1;
-        np += (d1 - wlo <= wspan) ? 1u : 0u;
+        col[fill * 32] = ((uint64_t)d0 << 32) | i0;
+        fill += (d0 - wlo <= wspan) ? 1u : 0u;
+        col[fill * 32] = ((uint64_t)d1 << 32) | i1;
+        fill += (d1 - wlo <= wspan) ? 1u : 0u;
       };
       // four staged candidates (slots c0..c0+3, c0 even): two pairs, two f32x2 chains
       auto test4_staged = [&](int c0) {
@@ -306,9 +325,11 @@ k_search(SearchArgs a) {
                   __float_as_uint(p3.w));
       };
       auto check = [&]() {
-        if (__any_sync(0xffffffffu, np > kPending - kCheck)) {
-          flush_pending(heap, pend, np, n, k, root, root_d, any_k);
-          hit_window(act && !(any_k && n >= k), lim_l, root_d, KNN, wlo, wspan);
+        if (__any_sync(0xffffffffu, fill > slots - kCheck)) {
+          top.fill = fill;
+          top = merge_column(col, top, k, any_k);
+          fill = top.fill;
+          hit_window(act && !(any_k && top.n >= k), lim_l, root_dist(top, k), KNN, wlo, wspan);
         }
       };
       uint32_t sc = 0;   // staged candidates (warp-uniform, < 32 between batches)
@@ -429,7 +450,9 @@ k_search(SearchArgs a) {
         __syncwarp();
       }
 
-      flush_pending(heap, pend, np, n, k, root, root_d, any_k);
+      top.fill = fill;
+      top = merge_column(col, top, k, any_k);
+      const uint32_t n = top.n;
       if (lane == 0 && loaded) {
         atomicAdd(&a.ctr->n_loaded, (unsigned long long)loaded);
         atomicAdd(&a.ctr->n_tested, (unsigned long long)tested);
@@ -440,10 +463,10 @@ k_search(SearchArgs a) {
       if (act) short_lane = incomplete;
       if (done && sorted_rows) {
         for (uint32_t i = 1; i < n; ++i) {
-          const uint64_t x = heap[i * 32];
+          const uint64_t x = col[i * 32];
           uint32_t j = i;
-          while (j > 0 && heap[(j - 1) * 32] > x) { heap[j * 32] = heap[(j - 1) * 32]; --j; }
-          heap[j * 32] = x;
+          while (j > 0 && col[(j - 1) * 32] > x) { col[j * 32] = col[(j - 1) * 32]; --j; }
+          col[j * 32] = x;
         }
       }
       __syncwarp();
@@ -504,21 +527,30 @@ cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, cons
   return cudaGetLastError();
 }
 
-size_t search_smem_bytes(uint32_t k, int warps_per_block) {
-  return (size_t)warps_per_block * (kStage * 16 + (size_t)(k + kPending) * 32 * 8);
+size_t search_smem_bytes(uint32_t k, uint32_t pending, int warps_per_block) {
+  return (size_t)warps_per_block * (kStage * 16 + (size_t)(k + pending) * 32 * 8);
+}
+
+void fit_search_shape(uint32_t k, uint32_t pending_req, int wpb_req, uint32_t* pending, int* wpb) {
+  uint32_t p = std::max(8u, std::min(256u, pending_req)) & ~3u;
+  while (p > 8 && search_smem_bytes(k, p, 1) > kSearchSmemLimit) p -= 4;
+  int w = std::max(1, std::min(8, wpb_req));
+  while (w > 1 && search_smem_bytes(k, p, w) > kSearchSmemLimit) --w;
+  *pending = p;
+  *wpb = w;
 }
 
 cudaError_t search_prepare(int device) {
   (void)device;
-  cudaError_t e = cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSearchSmemLimit);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    e = cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSearchSmemLimit);
   return e;
 }
 
-int search_blocks_per_sm(bool knn, uint32_t k, int warps_per_block) {
+int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block) {
   int nb = 0;
-  const size_t smem = search_smem_bytes(k, warps_per_block);
+  const size_t smem = search_smem_bytes(k, pending, warps_per_block);
   cudaError_t e = knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<true>, warps_per_block * 32, smem)
                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<false>, warps_per_block * 32, smem);
   if (e != cudaSuccess) return 1;
@@ -527,7 +559,7 @@ int search_blocks_per_sm(bool knn, uint32_t k, int warps_per_block) {
 
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
                           cudaStream_t s) {
-  const size_t smem = search_smem_bytes(a.k, warps_per_block);
+  const size_t smem = search_smem_bytes(a.k, a.pending, warps_per_block);
   if (knn) k_search<true><<<blocks, warps_per_block * 32, smem, s>>>(a);
   else k_search<false><<<blocks, warps_per_block * 32, smem, s>>>(a);
   return cudaGetLastError();

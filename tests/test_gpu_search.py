@@ -288,6 +288,28 @@ def test_walk_modes_give_identical_rows(ctx, ratio):
         ctx.set_tuning(**base)
 
 
+@pytest.mark.parametrize("slots", [8, 12, 32, 256])
+def test_pending_slots_give_identical_rows(ctx, slots):
+    """Few slots force many merges of appended hits into the kept K (some lanes at exactly
+    K kept when another lane's column fills); many slots merge once. Rows match the
+    oracle either way, for small and large K, with the partition on and off."""
+    base = ctx.tuning().as_dict()
+    try:
+        ctx.set_tuning(**{**base, "pending_slots": slots})
+        u = wl.uniform_cube(20_000, 40.0, seed=1)
+        for mode, k in (("knn", 5), ("knn", 64), ("radius", 7), ("radius", 128)):
+            exp = oracle.grid_search(u, None, mode, 3.0, k)
+            for part in (False, True):
+                got = ctx.search(u, None, mode, 3.0, k, partition=part)
+                assert_rows_equal(got, exp, sorted_rows=False)
+        p, off = wl.multicloud(n_clouds=16, lo=64, hi=4000, seed=3)
+        got = ctx.search_batched(p, off, mode="knn", radius=0.2, k=32, sorted_rows=True,
+                                 partition=True)
+        assert np.array_equal(got, oracle.grid_search_batched(p, off, mode="knn", r=0.2, k=32))
+    finally:
+        ctx.set_tuning(**base)
+
+
 def test_bounded_wait_reports_timeout_and_context_survives(ctx):
     """A device-side wait that can never be satisfied (a scan predecessor nobody
     publishes) gives up after its limit and reports RTNN_ERR_DEVICE_TIMEOUT; the context
