@@ -97,6 +97,7 @@ __device__ __forceinline__ float4 stage_get(const float* st, uint32_t slot) {
 
 constexpr int kCheck = 4;          // candidates tested between two buffer-full votes
 constexpr int kStage = 64;         // staged candidates per warp (float4)
+constexpr uint64_t kRowStride = 4294967311ull;   // prime > 2^32 > any row count of a box
 
 // Hit window on the bits of a non-negative FP32 distance d (bit order == value order):
 // radius: d < lim;  KNN: 0 < d < lim;  and, once the heap is full, d <= root distance
@@ -394,7 +395,13 @@ k_search(SearchArgs a) {
         uint32_t rs = 0, re = 0;
         const int ri = rb + lane;
         if (ri < nrows) {
-          const int cy = ly + ri % ny, cz = lz + ri / ny;
+          // rows in a scattered order (stride permutation: kRowStride is a prime above any
+          // row count, so i -> i * kRowStride mod nrows is a bijection of [0, nrows); the
+          // product stays below 2^63): a lane's hits are
+          // spread over the walk instead of arriving in one burst, which keeps the lanes'
+          // appended counts level and the merges short
+          const int rq = (int)(((uint64_t)ri * kRowStride) % (uint64_t)nrows);
+          const int cy = ly + rq % ny, cz = lz + rq / ny;
           const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
           rs = __ldg(a.cells + rowc + lx);
           re = __ldg(a.cells + rowc + hx + 1);
