@@ -158,8 +158,9 @@ typedef struct rtnn_tuning {
   uint32_t warps_per_block;   /* search kernel block size in warps (1..8) */
   uint32_t blocks_per_sm;     /* persistent search grid = SMs * blocks_per_sm (0: occupancy) */
   float width_margin;     /* learned width = margin * predicted K-th distance */
-  uint32_t fallback_passes;   /* partitioned search: passes that retry short queries at twice
-                                 their width before the last pass at the full radius (0..6) */
+  uint32_t fallback_passes;   /* partitioned search: passes that retry short queries at a wider
+                                 width (grown from the density each saw, 1.15x to 2x) before
+                                 the last pass at the full radius (0..6) */
   float lane_walk_ratio;      /* a 32-query tile whose extent exceeds ratio x its search width
                                  is searched lane by lane (each lane walks its own query's
                                  cells) instead of sharing one candidate stream; 0: never */

@@ -27,8 +27,8 @@ GRID_KNOBS = [
     ("pending_slots", [8, 16, 32, 64]),
 ]
 LEARNED_KNOBS = [
-    ("width_margin", [1.15, 1.3, 1.6]),
-    ("fallback_passes", [2, 4]),
+    ("width_margin", [1.0, 1.08, 1.15, 1.25, 1.4]),
+    ("fallback_passes", [2, 4, 6]),
 ]
 
 

@@ -398,8 +398,9 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   const uint64_t need_blocks = (sh.n_tiles + wpb - 1) / wpb;
   const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
   // pass 0: every query at its partition width; each pass flags its short queries, an
-  // order-preserving compaction (scan of the flags) turns them into list p%2 at twice
-  // the width, and escalation pass p reads list (p-1)%2; the final pass searches what
+  // order-preserving compaction (scan of the flags) turns them into list p%2 at a wider
+  // width (grown by the density each query saw, at most doubled), and escalation pass p
+  // reads list (p-1)%2; the final pass searches what
   // is left at the full radius. Lists stay in (cloud, bucket, Morton) order, so fallback
   // tiles remain spatially coherent.
   const int n_fb = part ? (int)fallback_passes_of(pr) : 0;

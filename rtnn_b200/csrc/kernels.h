@@ -24,8 +24,8 @@ struct SearchArgs {
   const uint32_t* fb_in_cloud;
   const float* fb_in_width;
   const uint32_t* fb_in_count;
-  // ... and flag each entry that is still short (flag per entry, and the doubled
-  // width it is retried at); nullptr in the final pass
+  // ... and flag each entry that is still short (flag per entry, and the wider width
+  // it is retried at); nullptr in the final pass
   uint32_t* fb_flag;
   float* fb_next_w;
   int32_t* out;                // [Q][k]
@@ -43,7 +43,7 @@ struct SearchArgs {
                                // than ratio * width (0: split at cloud changes only)
 };
 constexpr int kPassMain = 0;      // sorted queries, widths from the partition
-constexpr int kPassEscalate = 1;  // fallback list at its (doubled) widths
+constexpr int kPassEscalate = 1;  // fallback list at its (widened) widths
 constexpr int kPassFinal = 2;     // fallback list at the full radius (always complete)
 
 // scan.cu

@@ -464,10 +464,17 @@ k_search(SearchArgs a) {
         atomicAdd(&a.ctr->n_loaded, (unsigned long long)loaded);
         atomicAdd(&a.ctr->n_tested, (unsigned long long)tested);
       }
-      // completion: a narrowed search that found fewer than K neighbors is redone at r
+      // completion: a narrowed search that found fewer than K neighbors is redone wider.
+      // The next width assumes the local density it saw: n points within w means about
+      // K + 1 within w * cbrt((K + 1) / (n + 1)); a 10 % margin on that, at least 1.15 w
+      // (progress) and at most 2 w (a query that found nothing doubles)
       const bool incomplete = act && (lim_l < a.r2) && (n < k);
       const bool done = act && !incomplete;
       if (act) short_lane = incomplete;
+      if (incomplete && a.fb_next_w) {
+        const float grow = fminf(fmaxf(1.1f * cbrtf((k + 1.f) / (n + 1.f)), 1.15f), 2.f);
+        a.fb_next_w[entry] = fminf(grow * w, a.radius);
+      }
       if (done && sorted_rows) {
         for (uint32_t i = 1; i < n; ++i) {
           const uint64_t x = col[i * 32];
@@ -497,7 +504,6 @@ k_search(SearchArgs a) {
     // flag per entry; the compaction keeps the flagged ones in this pass's order
     if (a.fb_flag && in_range) {
       a.fb_flag[entry] = short_lane ? 1u : 0u;
-      if (short_lane) a.fb_next_w[entry] = fminf(2.f * w, a.radius);  // twice as wide next
     }
   }
 }
