@@ -406,43 +406,56 @@ k_search(SearchArgs a) {
           rs = __ldg(a.cells + rowc + lx);
           re = __ldg(a.cells + rowc + hx + 1);
         }
-        const int nr = min(32, nrows - rb);
-        for (int j = 0; j < nr; ++j) {
-          const uint32_t s0 = __shfl_sync(0xffffffffu, rs, j);
-          const uint32_t e0 = __shfl_sync(0xffffffffu, re, j);
-          for (uint32_t b = s0; b < e0; b += 32) {
-            // 3. stream 32 points, drop those farther than R from the box, compact the
-            //    survivors behind the ones already staged (rows accumulate)
-            const uint32_t idx = b + lane;
-            bool keep = false;
-            float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (idx < e0) {
-              p = __ldg(a.spts + idx);
-              const float ex = fmaxf(fmaxf(bx0 - p.x, p.x - bx1), 0.f);
-              const float ey = fmaxf(fmaxf(by0 - p.y, p.y - by1), 0.f);
-              const float ez = fmaxf(fmaxf(bz0 - p.z, p.z - bz1), 0.f);
-              keep = ex * ex + ey * ey + ez * ez <= R2k;
-            }
-            const uint32_t m = __ballot_sync(0xffffffffu, keep);
-            if (keep) stage_put(stage, sc + __popc(m & lt), p);
-            sc += __popc(m);
-            loaded += min(32u, e0 - b);
-            tested += __popc(m);
-            if (sc >= 32) {
-              __syncwarp();
+        // the (up to) 32 rows as one sequence of candidates: an inclusive scan of the row
+        // lengths; candidate t belongs to the row whose scanned end is the first above t
+        const uint32_t len = re - rs;
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t shift = rs - (incl - len);   // candidate t of this row: spts[t + shift]
+        for (uint32_t b = 0; b < total; b += 32) {
+          // 3. stream 32 candidates, drop those farther than R from the box, compact the
+          //    survivors behind the ones already staged (rows accumulate)
+          const uint32_t t = b + lane;
+          int row = 0;   // rows whose end is <= t (binary search over the lanes' ends)
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t e = __shfl_sync(0xffffffffu, incl, row + step - 1);
+            if (e <= t) row += step;
+          }
+          const uint32_t idx = t + __shfl_sync(0xffffffffu, shift, row);
+          bool keep = false;
+          float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (t < total) {
+            p = __ldg(a.spts + idx);
+            const float ex = fmaxf(fmaxf(bx0 - p.x, p.x - bx1), 0.f);
+            const float ey = fmaxf(fmaxf(by0 - p.y, p.y - by1), 0.f);
+            const float ez = fmaxf(fmaxf(bz0 - p.z, p.z - bz1), 0.f);
+            keep = ex * ex + ey * ey + ez * ez <= R2k;
+          }
+          const uint32_t m = __ballot_sync(0xffffffffu, keep);
+          if (keep) stage_put(stage, sc + __popc(m & lt), p);
+          sc += __popc(m);
+          loaded += min(32u, total - b);
+          tested += __popc(m);
+          if (sc >= 32) {
+            __syncwarp();
 #pragma unroll 2
-              for (int c0 = 0; c0 < 32; c0 += kCheck) {
-                test4_staged(c0);
-                check();
-              }
-              __syncwarp();
-              sc -= 32;
-              float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
-              if (lane < sc) carry = stage_get(stage, 32 + lane);
-              __syncwarp();
-              if (lane < sc) stage_put(stage, lane, carry);
-              __syncwarp();
+            for (int c0 = 0; c0 < 32; c0 += kCheck) {
+              test4_staged(c0);
+              check();
             }
+            __syncwarp();
+            sc -= 32;
+            float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (lane < sc) carry = stage_get(stage, 32 + lane);
+            __syncwarp();
+            if (lane < sc) stage_put(stage, lane, carry);
+            __syncwarp();
           }
         }
       }
