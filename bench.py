@@ -37,7 +37,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per query of the main search pass, from the ncu capture in
 # profiles/k_search_knn_multicloud_scale0.1.md (866 MB for 5.25 M queries), scaled by
 # queries to a full launch; only known for the default workload.
-TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 165.0}
+TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 160.0}
 
 
 def parse():
@@ -66,7 +66,8 @@ def run_profile(args):
     cfg = make_workload(args.workload, args.scale, 0)
     ctx = rtnn_b200.Context(0)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
-    ctx.set_tuning(points_per_cell=1.0, width_margin=1.3, fallback_passes=4)
+    ctx.set_tuning(points_per_cell=1.0, cell_ratio=0.5, width_margin=1.1, fallback_passes=6,
+                   gap_ratio=2.0, pending_slots=8)
     train_model(ctx, cfg, args.scale, 0)
     tp = torch.from_numpy(cfg["points"]).cuda()
     tq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).cuda()
