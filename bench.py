@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per query of the main search pass, from the ncu capture in
-# profiles/k_search_knn_multicloud_scale0.1.md (866 MB for 5.25 M queries), scaled by
+# profiles/k_search_knn_multicloud_scale0.1.md (839 MB for 5.25 M queries), scaled by
 # queries to a full launch; only known for the default workload.
 TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 160.0}
 
