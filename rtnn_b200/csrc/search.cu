@@ -514,6 +514,12 @@ k_search(SearchArgs a) {
       }
       __syncwarp();
     }
+    // a query that cannot be searched (a non-finite coordinate) gets an empty row
+    for (uint32_t m = __ballot_sync(0xffffffffu, in_range && !valid); m; m &= m - 1) {
+      const int L = __ffs(m) - 1;
+      const uint32_t qi = __float_as_uint(__shfl_sync(0xffffffffu, q.w, L));
+      for (uint32_t jj = lane; jj < k; jj += 32) a.out[(size_t)qi * k + jj] = -1;
+    }
     // flag per entry; the compaction keeps the flagged ones in this pass's order
     if (a.fb_flag && in_range) {
       a.fb_flag[entry] = short_lane ? 1u : 0u;

@@ -165,6 +165,22 @@ def test_far_and_nonfinite_queries(ctx):
     assert np.array_equal(got[4:], exp)
 
 
+def test_nonfinite_query_rows_are_written(ctx):
+    """Rows of queries that cannot be searched (NaN or infinite coordinates) are filled
+    with -1 by the search itself, whatever the output buffer held before."""
+    import torch
+    p = wl.uniform_cube(3000, 10.0, seed=3)
+    q = np.array([[np.nan, 1, 1], [1, np.inf, 1], [5, 5, 5], [1, 1, -np.inf]], np.float32)
+    tp, tq = torch.from_numpy(p).cuda(), torch.from_numpy(q).cuda()
+    for mode in ("knn", "radius"):
+        for part in (False, True):
+            out = torch.full((4, 6), 7, dtype=torch.int32, device="cuda")
+            ctx.search(tp, tq, mode, 2.0, 6, partition=part, sorted_rows=True, out=out)
+            got = out.cpu().numpy()
+            assert (got[[0, 1, 3]] == -1).all(), got
+            assert np.array_equal(got[2], oracle.bruteforce(p, q[2:3], mode, 2.0, 6)[0])
+
+
 def test_invalid_arguments(ctx):
     p = wl.uniform_cube(10, 1.0, seed=0)
     with pytest.raises(rtnn_b200.RtnnError) as e:
