@@ -382,18 +382,17 @@ def run_rtnn(args, rank, world):
     # the plain grid search (full radius for every query), with its own best tuning
     plain_ms, plain_tuning, result_plain = None, None, None
     if not args.no_plain:
-        plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, use_cache=False, **common)
+        plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, presets=at.GRID_PRESETS,
+                                   use_cache=False, **common)
         plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
         plain_ms, _ = timed(plain, args.steps, max(1, args.warmup // 2))
         plain.close()
 
-    # learned partition: grid knobs tuned on the analytic partition, the width model
-    # trained on clouds of other seeds at that tuning, then margin / fallback passes
+    # learned partition: for each cell-size preset the width model is trained on clouds of
+    # other seeds at that grid and the margin tuned; the best preset is then tuned further
     ctx.set_tuning(**base_tuning)
-    at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, partition=True, use_cache=False, **common)
-    model_info = train_model(ctx, cfg, args.scale, rank)
-    learned_tuning = at.autotune(ctx, *wl_args, knobs=at.LEARNED_KNOBS, learned=True,
-                                 use_cache=False, **common)
+    learned_tuning, model_info = at.autotune_learned(
+        ctx, *wl_args, train=lambda c: train_model(c, cfg, args.scale, rank), **common)
     learned = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=True, **common)
     ms_learned, clocks = timed(learned, args.steps, args.warmup, ClockSampler(dev))
     st = rtnn_b200.Stats()

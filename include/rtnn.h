@@ -172,6 +172,13 @@ typedef struct rtnn_tuning {
                                  merge into its K kept neighbors (8..256); more slots mean
                                  fewer merges and fewer resident warps. Reduced when K +
                                  slots would not fit one warp's shared memory */
+  uint32_t query_warps;       /* search kernel: 0: one warp per 32-query tile sharing one
+                                 candidate stream (wide widths, coherent queries); 1: one
+                                 warp per query -- each query walks only its own candidate
+                                 box and keeps its hits with warp-wide sorts (narrow widths);
+                                 2: tiles for the first pass, one warp per query for the
+                                 escalation passes (scattered short queries). K <= 64 for
+                                 the per-query kernel; larger K always use the tiles */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

@@ -2,9 +2,10 @@
 
 Picks the tuning knobs of a context (include/rtnn.h, rtnn_tuning) for one workload by
 timing candidate settings on the GPU with the library's own event timers, one knob at a
-time (coordinate descent): the cell edge (points per cell for dense clouds, cell/radius
-ratio), the search block size (warps per block), and -- for the learned partition -- the
-width margin and the number of doubling fallback passes. Choices are cached in a JSON file
+time (coordinate descent) after timing a few whole cell-size presets: the cell edge
+(points per cell for dense clouds, cell/radius ratio), the search kernels (tiles or one
+warp per query, block size, run splitting, result-column slots), and -- for the learned
+partition -- the width margin and the number of escalation passes. Choices are cached in a JSON file
 keyed by a workload signature (sizes, cloud count, mode, r, K, flags, GPU name), so later
 runs of the same kind of workload skip the search.
 
@@ -18,13 +19,26 @@ import numpy as np
 
 import rtnn_b200
 
-GRID_KNOBS = [
-    ("points_per_cell", [0.0, 1.0, 4.0, 16.0]),
-    ("cell_ratio", [0.5, 1.0]),
+# knobs that change the grid (and so the learned model's input features)
+CELL_KNOBS = [
+    ("points_per_cell", [0.0, 0.25, 1.0, 4.0, 16.0]),
+    ("cell_ratio", [0.25, 0.5, 1.0]),
+]
+# knobs of the search kernels only
+SEARCH_KNOBS = [
     ("warps_per_block", [2, 4]),
     ("lane_walk_ratio", [0.0, 0.5, 1.0, 2.0]),
     ("gap_ratio", [0.0, 1.0, 2.0, 4.0]),
     ("pending_slots", [8, 16, 32, 64]),
+    ("query_warps", [0, 1, 2]),
+]
+GRID_KNOBS = CELL_KNOBS + SEARCH_KNOBS
+# whole cell-size regimes tried as starting points: one knob at a time would not move from
+# coarse cells with tiles to fine cells with per-query escalation passes
+GRID_PRESETS = [
+    {"cell_ratio": 0.5, "min_cell_ratio": 0.0625, "points_per_cell": 1.0, "query_warps": 0},
+    {"cell_ratio": 0.25, "min_cell_ratio": 0.02, "points_per_cell": 0.25, "query_warps": 2},
+    {"cell_ratio": 1.0, "min_cell_ratio": 0.0625, "points_per_cell": 4.0, "query_warps": 0},
 ]
 LEARNED_KNOBS = [
     ("width_margin", [1.0, 1.08, 1.15, 1.25, 1.4]),
@@ -81,9 +95,10 @@ def time_plan(ctx, points, offsets, queries, qoffsets, out, repeats=2, **plan_kw
 
 
 def autotune(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radius=0.2, k=32,
-             partition=False, learned=False, knobs=None, use_cache=True, log=None):
+             partition=False, learned=False, knobs=None, presets=None, use_cache=True, log=None):
     """Tunes `ctx` for this workload (CUDA tensors, host offset arrays). Returns the
-    chosen tuning as a dict and leaves it set on the context."""
+    chosen tuning as a dict and leaves it set on the context. `presets` (partial tunings)
+    are timed first and the best one is the starting point of the descent."""
     import torch
     offsets = np.asarray(offsets, dtype=np.uint64)
     n_clouds = len(offsets) - 1
@@ -99,6 +114,19 @@ def autotune(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radi
     best = ctx.tuning().as_dict()
     best_ms = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
     trials = [(dict(best), best_ms)]
+    for pre in presets or []:
+        cand = {**best, **pre}
+        try:
+            ctx.set_tuning(**cand)
+        except rtnn_b200.RtnnError:
+            continue
+        ms = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
+        trials.append((dict(cand), ms))
+        if log:
+            log(f"autotune preset {pre}: {ms:.3f} ms (best {best_ms:.3f})")
+        if ms < best_ms:
+            best, best_ms = cand, ms
+    ctx.set_tuning(**best)
     for name, values in knobs:
         for v in values:
             if best.get(name) == v:
@@ -120,3 +148,36 @@ def autotune(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radi
     if use_cache:
         _save(cache)
     return best
+
+
+def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radius=0.2,
+                     k=32, train=None, presets=None, log=None):
+    """Tuning for the learned partition. The width model's features depend on the grid, so
+    for every cell-size preset the model is trained at that grid (`train(ctx)` collects
+    training data and trains; what it returns is handed back for the chosen preset) and
+    the width margin is tuned; the best preset's model is kept, then the search and
+    learned knobs, which leave the grid alone, are tuned by descent.
+    Returns (tuning, train's result for the chosen preset)."""
+    import torch
+    offsets = np.asarray(offsets, dtype=np.uint64)
+    nq = int(offsets[-1]) if queries is None else int(np.asarray(qoffsets)[-1])
+    out = torch.empty((nq, k), dtype=torch.int32, device=points.device)
+    kw = dict(mode=mode, radius=radius, k=k, learned=True)
+    start = ctx.tuning().as_dict()
+    best = None
+    for pre in presets if presets is not None else GRID_PRESETS:
+        ctx.set_tuning(**{**start, **pre})
+        info = train(ctx)
+        tun = autotune(ctx, points, offsets, queries, qoffsets,
+                       knobs=[("width_margin", [1.0, 1.1, 1.25])], use_cache=False, log=log, **kw)
+        ms = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
+        if log:
+            log(f"autotune learned preset {pre}: {ms:.3f} ms")
+        if best is None or ms < best[0]:
+            best = (ms, tun, ctx.get_model(), info)
+    _, tun, model, info = best
+    ctx.set_tuning(**tun)
+    ctx.set_model(model)
+    tun = autotune(ctx, points, offsets, queries, qoffsets, knobs=SEARCH_KNOBS + LEARNED_KNOBS,
+                   use_cache=False, log=log, **kw)
+    return tun, info

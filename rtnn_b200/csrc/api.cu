@@ -101,7 +101,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f, 16u};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f, 16u, 0u};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
@@ -392,11 +392,22 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
             ((pr.flags & RTNN_FLAG_ANY_K) ? kSearchAnyK : 0u);
   int wpb = 4;
   fit_search_shape(pr.k, tu.pending_slots, (int)tu.warps_per_block, &a.pending, &wpb);
-  int bps = search_blocks_per_sm(knn, pr.k, a.pending, wpb);
-  if (tu.blocks_per_sm > 0) bps = std::min(bps, (int)tu.blocks_per_sm);
-  const uint64_t persistent = (uint64_t)c->n_sms * bps;
-  const uint64_t need_blocks = (sh.n_tiles + wpb - 1) / wpb;
-  const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
+  a.qcap = search_q_cap(pr.k);   // 0: k too large for one warp's hit buffer
+  // kernel per pass: the tile walk, or one warp per query (query_warps 1: every pass;
+  // 2: the escalation passes only, whose short queries are scattered over the clouds)
+  const bool q_main = tu.query_warps == 1 && a.qcap != 0;
+  const bool q_fallback = tu.query_warps != 0 && a.qcap != 0;
+  const int wpb_q = (int)std::max(1u, std::min(8u, tu.warps_per_block));
+  auto grid_for = [&](bool per_query, int w) {
+    int bps = per_query ? search_q_blocks_per_sm(knn, pr.k, w)
+                        : search_blocks_per_sm(knn, pr.k, a.pending, w);
+    if (tu.blocks_per_sm > 0) bps = std::min(bps, (int)tu.blocks_per_sm);
+    const uint64_t persistent = (uint64_t)c->n_sms * bps;
+    const uint64_t need_blocks = (sh.n_tiles + w - 1) / w;
+    return (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
+  };
+  const unsigned blocks_tile = grid_for(false, wpb);
+  const unsigned blocks_q = a.qcap != 0 ? grid_for(true, wpb_q) : 1u;
   // pass 0: every query at its partition width; each pass flags its short queries, an
   // order-preserving compaction (scan of the flags) turns them into list p%2 at a wider
   // width (grown by the density each query saw, at most doubled), and escalation pass p
@@ -418,7 +429,10 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     a.fb_flag = flagging ? flags : nullptr;
     a.fb_next_w = flagging ? (float*)ws.fbnextw.p : nullptr;
     if (flagging) RTNN_CU(cudaMemsetAsync(flags, 0, (sh.Q + 1) * 4, s), "memset flags");
-    RTNN_CU(launch_search(knn, a, blocks, wpb, s), p == 0 ? "search" : "fallback search");
+    const bool per_query = p == 0 ? q_main : q_fallback;
+    RTNN_CU(per_query ? launch_search_q(knn, a, blocks_q, wpb_q, s)
+                      : launch_search(knn, a, blocks_tile, wpb, s),
+            p == 0 ? "search" : "fallback search");
     if (flagging) {
       const uint32_t* n_dev = p > 0 ? &ctr->fb_count[p - 1] : nullptr;
       RTNN_CU(launch_scan_excl(flags, sh.Q + 1, n_dev, 1, sh.Q + 1, (uint64_t*)ws.scan_state.p,
@@ -605,7 +619,7 @@ rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
       !(t->points_per_cell >= 0.f) || t->fallback_passes > kMaxPasses - 2 ||
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f) ||
       !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f) || t->pending_slots < 8 ||
-      t->pending_slots > 256)
+      t->pending_slots > 256 || t->query_warps > 2)
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
   return RTNN_OK;

@@ -36,6 +36,7 @@ struct SearchArgs {
   float r2;                    // fl(r * r)
   uint32_t k;
   uint32_t pending;            // appended-hit slots per lane beyond the k kept ones
+  uint32_t qcap;               // k_search_q: hit buffer entries per warp (search_q_cap)
   uint32_t flags;              // kSearch*
   int pass;                    // kPassMain, kPassEscalate or kPassFinal
   float lane_walk_ratio;       // tile spread > ratio * width: per-lane walk (0: never)
@@ -91,6 +92,11 @@ cudaError_t search_prepare(int device);
 int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block);
 // appended-hit slots (multiple of 4, 8..256) and warps per block that fit the limit
 void fit_search_shape(uint32_t k, uint32_t pending_req, int wpb_req, uint32_t* pending, int* wpb);
+// one warp per query (k_search_q): buffer size for k, occupancy and launch
+uint32_t search_q_cap(uint32_t k);
+int search_q_blocks_per_sm(bool knn, uint32_t k, int warps_per_block);
+cudaError_t launch_search_q(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
+                            cudaStream_t s);
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
                           cudaStream_t s);
 cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, const uint32_t* n_dev,

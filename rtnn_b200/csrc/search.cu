@@ -96,6 +96,7 @@ __device__ __forceinline__ float4 stage_get(const float* st, uint32_t slot) {
 }
 
 constexpr int kCheck = 4;          // candidates tested between two buffer-full votes
+constexpr uint32_t kQueryCap = 128;   // k_search_q hit buffer per warp (k <= 64)
 constexpr int kStage = 64;         // staged candidates per warp (float4)
 constexpr uint64_t kRowStride = 4294967311ull;   // prime > 2^32 > any row count of a box
 
@@ -527,6 +528,264 @@ k_search(SearchArgs a) {
   }
 }
 
+// ---- one warp per query ---------------------------------------------------------------
+// The alternative walk for narrow widths: a warp takes a tile of 32 sorted queries like
+// k_search but searches them one after another, each over its own candidate box only
+// (a tile box holds many times more points than the box of one of its queries). The
+// box's cell rows are flattened 64 candidates at a time, two per lane (prefix sum of the
+// row lengths, shuffle search for a candidate's row), every lane tests its candidates
+// against the query, and the hits are compacted into a per-warp buffer in shared memory
+// with ballots. When the buffer could overflow, and at the end when it holds more than
+// K, a warp-wide bitonic sort keeps the K nearest; the sorted buffer is then the row.
+
+// Sorts buf[0, n) ascending with the whole warp (n <= 32 E, E <= 4; position e * 32 + lane, E per
+// lane, padding ~0 sorts last), writes the first `keep` (1 <= keep <= n) back to
+// buf[0, keep) and returns the key at sorted position keep - 1.
+template <int E>
+__device__ __forceinline__ uint64_t warp_sort_keep(uint64_t* buf, uint32_t n, uint32_t keep) {
+  const int lane = threadIdx.x & 31;
+  uint64_t v[E];
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const uint32_t p = (uint32_t)(e * 32 + lane);
+    v[e] = p < n ? buf[p] : ~0ull;
+  }
+  // loops over log2(size) and log2(stride): constant trip counts, fully unrolled, so v[]
+  // stays in registers
+  constexpr int kLog = E == 1 ? 5 : E == 2 ? 6 : 7;
+#pragma unroll
+  for (int ls = 1; ls <= kLog; ++ls) {
+    const int size = 1 << ls;
+#pragma unroll
+    for (int lt = ls - 1; lt >= 0; --lt) {
+      const int stride = 1 << lt;
+      if (stride >= 32) {   // partner in this lane; size >= 64, so the direction is e's
+        const int es = stride >> 5;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          if (e & es) continue;
+          const bool up = ((e * 32) & size) == 0;
+          const uint64_t x = v[e], y = v[e | es];
+          const bool sw = up ? (x > y) : (x < y);
+          v[e] = sw ? y : x;
+          v[e | es] = sw ? x : y;
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const uint64_t o = __shfl_xor_sync(0xffffffffu, v[e], stride);
+          const bool up = ((uint32_t)(e * 32 + lane) & (uint32_t)size) == 0;
+          const bool low = (lane & stride) == 0;
+          const uint64_t lo = v[e] < o ? v[e] : o, hi = v[e] < o ? o : v[e];
+          v[e] = (low == up) ? lo : hi;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  uint64_t kth = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const uint32_t p = (uint32_t)(e * 32 + lane);
+    if (p < keep) buf[p] = v[e];
+    if (e == (int)((keep - 1) >> 5)) kth = v[e];
+  }
+  __syncwarp();
+  return __shfl_sync(0xffffffffu, kth, (int)((keep - 1) & 31));
+}
+
+// Keeps the `keep` smallest of buf[0, n) (n <= 128; sorted, at buf[0, keep)); the sort is
+// sized to n. Out of line: one call target keeps the query loop's registers and code small.
+__device__ __noinline__ uint64_t warp_select(uint64_t* buf, uint32_t n, uint32_t keep) {
+  if (n <= 32) return warp_sort_keep<1>(buf, n, keep);
+  if (n <= 64) return warp_sort_keep<2>(buf, n, keep);
+  return warp_sort_keep<4>(buf, n, keep);
+}
+
+template <bool KNN>
+__global__ void __launch_bounds__(256, 2)
+k_search_q(SearchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t cap = a.qcap;   // hit buffer entries per warp: k + 64 <= cap = 128
+  uint64_t* buf = reinterpret_cast<uint64_t*>(smem) + (size_t)warp * cap;
+  const uint32_t lt = lanemask_lt();
+  const uint32_t k = a.k;
+  const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
+  const bool local_idx = (a.flags & kSearchLocalIndices) != 0;
+  const bool any_k = (a.flags & kSearchAnyK) != 0;
+  const bool main_pass = a.pass == kPassMain;
+  const uint32_t fb_total = main_pass ? 0u : *a.fb_in_count;
+  const uint32_t n_tiles = main_pass ? a.n_tiles : (fb_total + 31) / 32;
+  const uint32_t total_cells = a.ctr->total_cells;
+  unsigned long long loaded = 0, lane_tests = 0;   // work counters of this warp
+
+  while (true) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.work, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= n_tiles) break;
+
+    // this lane's query of the tile (the same fetch as k_search)
+    bool valid;
+    uint32_t pos, cloud, entry;
+    float wq = a.radius;
+    if (main_pass) {
+      uint32_t c = 0;
+      if (lane == 0) c = find_cloud(a.t.tile_base, a.t.n_clouds, tile);
+      cloud = __shfl_sync(0xffffffffu, c, 0);
+      pos = a.t.query_off[cloud] + (tile - a.t.tile_base[cloud]) * 32u + lane;
+      entry = pos;
+      valid = pos < a.t.query_off[cloud + 1];
+      if (valid && a.qwidth) wq = a.qwidth[pos];
+    } else {
+      entry = tile * 32u + lane;
+      valid = entry < fb_total;
+      pos = valid ? a.fb_in_pos[entry] : 0u;
+      cloud = valid ? a.fb_in_cloud[entry] : 0u;
+      if (valid && a.pass == kPassEscalate) wq = a.fb_in_width[entry];
+    }
+    const bool in_range = valid;
+    const float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float w = a.radius, lim = a.r2;
+    if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
+    valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
+    bool short_lane = false;
+
+    for (uint32_t todo = __ballot_sync(0xffffffffu, in_range); todo; todo &= todo - 1) {
+      const int j = __ffs(todo) - 1;
+      const float qx = __shfl_sync(0xffffffffu, q.x, j), qy = __shfl_sync(0xffffffffu, q.y, j);
+      const float qz = __shfl_sync(0xffffffffu, q.z, j);
+      const uint32_t qi = __float_as_uint(__shfl_sync(0xffffffffu, q.w, j));
+      const float wj = __shfl_sync(0xffffffffu, w, j), limj = __shfl_sync(0xffffffffu, lim, j);
+      const uint32_t cj = __shfl_sync(0xffffffffu, cloud, j);
+      const uint32_t ej = __shfl_sync(0xffffffffu, entry, j);
+      const bool vj = __shfl_sync(0xffffffffu, valid ? 1u : 0u, j) != 0u;
+      int32_t* row = a.out + (size_t)qi * k;
+      if (!vj) {   // a non-finite coordinate: nothing to search, an empty row
+        for (uint32_t jj = lane; jj < k; jj += 32) row[jj] = -1;
+        continue;
+      }
+      const CloudGrid g = a.grids[cj];
+      const bool grid_ok = (uint64_t)g.cell_base + g.n_cells <= (uint64_t)total_cells;
+      // candidate cells: the query's box +- R (R widened so every point whose rounded
+      // FP32 distance passes is inside)
+      const float R = __fmul_ru(wj, 1.000001f);
+      const float fx0 = cell_coord_f(__fsub_rn(qx, R), g.ox, g.inv_cell);
+      const float fx1 = cell_coord_f(__fadd_rn(qx, R), g.ox, g.inv_cell);
+      const float fy0 = cell_coord_f(__fsub_rn(qy, R), g.oy, g.inv_cell);
+      const float fy1 = cell_coord_f(__fadd_rn(qy, R), g.oy, g.inv_cell);
+      const float fz0 = cell_coord_f(__fsub_rn(qz, R), g.oz, g.inv_cell);
+      const float fz1 = cell_coord_f(__fadd_rn(qz, R), g.oz, g.inv_cell);
+      const bool empty = !(grid_ok && fx0 <= (float)(g.dx - 1) && fx1 >= 0.f &&
+                           fy0 <= (float)(g.dy - 1) && fy1 >= 0.f && fz0 <= (float)(g.dz - 1) &&
+                           fz1 >= 0.f);
+      const int lx = (int)fmaxf(fx0, 0.f), hx = (int)fminf(fx1, (float)(g.dx - 1));
+      const int ly = (int)fmaxf(fy0, 0.f), hy = (int)fminf(fy1, (float)(g.dy - 1));
+      const int lz = (int)fmaxf(fz0, 0.f), hz = (int)fminf(fz1, (float)(g.dz - 1));
+      const int ny = hy - ly + 1, nz = hz - lz + 1;
+      const int nrows = empty ? 0 : ny * nz;
+
+      uint32_t wlo, wspan;   // hit window on the distance bits (see hit_window)
+      hit_window(true, limj, INFINITY, KNN, wlo, wspan);
+      uint32_t nb = 0;       // hits in the buffer (warp-uniform)
+      bool stop = false;     // any_k: k hits found
+      for (int rb = 0; rb < nrows && !stop; rb += 32) {
+        uint32_t rs = 0, re = 0;
+        const int ri = rb + lane;
+        if (ri < nrows) {
+          const int cy = ly + ri % ny, cz = lz + ri / ny;
+          const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+          rs = __ldg(a.cells + rowc + lx);
+          re = __ldg(a.cells + rowc + hx + 1);
+        }
+        const uint32_t len = re - rs;
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t shift = rs - (incl - len);   // candidate t of this row: spts[t + shift]
+        // two candidates per lane per step (t and t + 32): independent lookups, loads and
+        // distances for the latency to overlap
+        for (uint32_t b = 0; b < total; b += 64) {
+          const uint32_t t0 = b + lane, t1 = b + 32 + lane;
+          int r0 = 0, r1 = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t e0 = __shfl_sync(0xffffffffu, incl, r0 + step - 1);
+            const uint32_t e1 = __shfl_sync(0xffffffffu, incl, r1 + step - 1);
+            if (e0 <= t0) r0 += step;
+            if (e1 <= t1) r1 += step;
+          }
+          const uint32_t idx0 = t0 + __shfl_sync(0xffffffffu, shift, r0);
+          const uint32_t idx1 = t1 + __shfl_sync(0xffffffffu, shift, r1);
+          bool hit0 = false, hit1 = false;
+          uint64_t key0 = 0, key1 = 0;
+          const float4 p0 = t0 < total ? __ldg(a.spts + idx0) : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 p1 = t1 < total ? __ldg(a.spts + idx1) : make_float4(0.f, 0.f, 0.f, 0.f);
+          if (t0 < total) {
+            const uint32_t d = __float_as_uint(dist2_ref(qx, qy, qz, p0.x, p0.y, p0.z));
+            hit0 = d - wlo <= wspan;
+            key0 = ((uint64_t)d << 32) | __float_as_uint(p0.w);
+          }
+          if (t1 < total) {
+            const uint32_t d = __float_as_uint(dist2_ref(qx, qy, qz, p1.x, p1.y, p1.z));
+            hit1 = d - wlo <= wspan;
+            key1 = ((uint64_t)d << 32) | __float_as_uint(p1.w);
+          }
+          const uint32_t m0 = __ballot_sync(0xffffffffu, hit0);
+          const uint32_t m1 = __ballot_sync(0xffffffffu, hit1);
+          if (hit0) buf[nb + __popc(m0 & lt)] = key0;
+          nb += __popc(m0);
+          if (hit1) buf[nb + __popc(m1 & lt)] = key1;
+          nb += __popc(m1);
+          const uint32_t took = min(64u, total - b);
+          loaded += took;
+          lane_tests += took;
+          if (any_k) {
+            if (nb >= k) { stop = true; break; }
+          } else if (nb > cap - 64) {
+            // keep the k nearest; later hits must beat the k-th (ties may win on index)
+            const uint64_t kth = warp_select(buf, nb, k);
+            nb = k;
+            hit_window(true, limj, __uint_as_float((uint32_t)(kth >> 32)), KNN, wlo, wspan);
+          }
+        }
+      }
+      const uint32_t found = min(nb, k);
+      const bool incomplete = (limj < a.r2) && (found < k);
+      if (lane == j) short_lane = incomplete;
+      if (incomplete) {
+        if (a.fb_next_w && lane == 0) {
+          // the next width assumes the local density this search saw (as in k_search)
+          const float grow = fminf(fmaxf(1.1f * cbrtf((k + 1.f) / (found + 1.f)), 1.15f), 2.f);
+          a.fb_next_w[ej] = fminf(grow * wj, a.radius);
+        }
+        continue;
+      }
+      if (any_k) {   // the first k found, in the order found (sorted on request)
+        if (sorted_rows && found > 1) warp_select(buf, found, found);
+      } else if (nb > k || (sorted_rows && nb > 1)) {
+        warp_select(buf, nb, found);
+      }
+      __syncwarp();
+      const uint32_t sub = local_idx ? a.t.point_off[cj] : 0u;
+      for (uint32_t jj = lane; jj < k; jj += 32)
+        row[jj] = jj < found ? (int32_t)((uint32_t)buf[jj] - sub) : -1;
+      __syncwarp();
+    }
+    if (a.fb_flag && in_range) a.fb_flag[entry] = short_lane ? 1u : 0u;
+  }
+  if (lane == 0 && loaded) {
+    atomicAdd(&a.ctr->n_loaded, loaded);
+    atomicAdd(&a.ctr->n_tested, (lane_tests + 31) / 32);
+  }
+}
+
 // Order-preserving compaction of the short queries of a pass: flags were scanned in
 // place (n + 1 entries, flags[n] = total), entry e is short when flags[e+1] > flags[e].
 __global__ void k_compact_fallback(const uint32_t* __restrict__ flags, uint32_t n_host,
@@ -587,6 +846,29 @@ int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_b
                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<false>, warps_per_block * 32, smem);
   if (e != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
+}
+
+size_t search_q_smem_bytes(uint32_t qcap, int warps_per_block) {
+  return (size_t)warps_per_block * qcap * 8;
+}
+
+uint32_t search_q_cap(uint32_t k) { return k + 64 <= kQueryCap ? kQueryCap : 0u; }
+
+int search_q_blocks_per_sm(bool knn, uint32_t k, int warps_per_block) {
+  int nb = 0;
+  const size_t smem = search_q_smem_bytes(search_q_cap(k), warps_per_block);
+  cudaError_t e = knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<true>, warps_per_block * 32, smem)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<false>, warps_per_block * 32, smem);
+  if (e != cudaSuccess) return 1;
+  return nb > 0 ? nb : 1;
+}
+
+cudaError_t launch_search_q(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
+                            cudaStream_t s) {
+  const size_t smem = search_q_smem_bytes(a.qcap, warps_per_block);
+  if (knn) k_search_q<true><<<blocks, warps_per_block * 32, smem, s>>>(a);
+  else k_search_q<false><<<blocks, warps_per_block * 32, smem, s>>>(a);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,

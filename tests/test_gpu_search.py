@@ -326,6 +326,40 @@ def test_pending_slots_give_identical_rows(ctx, slots):
         ctx.set_tuning(**base)
 
 
+@pytest.mark.parametrize("qw", [1, 2])
+@pytest.mark.parametrize("k", [1, 5, 32, 64, 96, 128])
+def test_query_warps_match_oracle(ctx, k, qw):
+    """One warp per query (query_warps 1: every pass; 2: escalation passes only; K > 64
+    falls back to the tile walk): rows equal the oracle's, sorted and as sets, with the
+    partition off and on (escalation passes included), in batched clouds, and with ANY_K."""
+    base = ctx.tuning().as_dict()
+    try:
+        ctx.set_tuning(**{**base, "query_warps": qw})
+        u = wl.uniform_cube(20_000, 40.0, seed=5)
+        for mode in ("knn", "radius"):
+            exp = oracle.grid_search(u, None, mode, 3.0, k)
+            assert np.array_equal(ctx.search(u, None, mode, 3.0, k, sorted_rows=True), exp)
+            for part in (False, True):
+                assert_rows_equal(ctx.search(u, None, mode, 3.0, k, partition=part), exp, False)
+            anyk = ctx.search(u, None, mode, 3.0, k, any_k=True)
+            n_exp = (exp >= 0).sum(1)
+            assert np.array_equal((anyk >= 0).sum(1), n_exp)
+            for qi in range(0, u.shape[0], 211):
+                g = anyk[qi][anyk[qi] >= 0]
+                assert len(set(g.tolist())) == len(g)
+        p, off = wl.multicloud(n_clouds=16, lo=64, hi=4000, seed=8)
+        got = ctx.search_batched(p, off, mode="knn", radius=0.2, k=min(k, 32), sorted_rows=True,
+                                 partition=True)
+        assert np.array_equal(got, oracle.grid_search_batched(p, off, mode="knn", r=0.2,
+                                                              k=min(k, 32)))
+        q = np.array([[np.nan, 1, 1], [20, 20, 20], [1e9, 0, 0]], np.float32)
+        got = ctx.search(u, q, "knn", 3.0, k, sorted_rows=True)
+        assert (got[[0, 2]] == -1).all()
+        assert np.array_equal(got[1], oracle.bruteforce(u, q[1:2], "knn", 3.0, k)[0])
+    finally:
+        ctx.set_tuning(**base)
+
+
 def test_bounded_wait_reports_timeout_and_context_survives(ctx):
     """A device-side wait that can never be satisfied (a scan predecessor nobody
     publishes) gives up after its limit and reports RTNN_ERR_DEVICE_TIMEOUT; the context
