@@ -342,6 +342,9 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     w.grids = grids;
     w.cells = cells;
     w.xyz = d_qs;
+    // self-search: queries taken in cell order (neighbours share their row reads); widths
+    // and training features are still written at the caller's query index
+    w.spts = d_qs == d_pts ? (const float4*)ws.spts.p : nullptr;
     w.total_cells = &ctr->total_cells;
     w.n_queries = (uint32_t)sh.Q;
     w.radius = pr.radius;

@@ -120,6 +120,8 @@ struct WidthArgs {
   const CloudGrid* grids;
   const uint32_t* cells;
   const float* xyz;             // queries in the caller's order (AoS float3)
+  const float4* spts;           // when the queries are the points: the cell-sorted points,
+                                // walked instead of xyz (nullptr: walk xyz)
   const uint32_t* total_cells;  // cells in use (device)
   uint32_t n_queries;
   float radius;

@@ -62,19 +62,31 @@ __device__ __forceinline__ float mlp_forward_norm(const MlpView& m, const float*
   return o;
 }
 
-// Box count of cells [cx-s, cx+s] x [cy-s, cy+s] x [cz-s, cz+s] clipped to the grid.
-__device__ __forceinline__ uint32_t box_count(const CloudGrid& g, const uint32_t* cells,
-                                              int cx, int cy, int cz, int s) {
-  const int x0 = max(cx - s, 0), x1 = min(cx + s, g.dx - 1);
-  const int y0 = max(cy - s, 0), y1 = min(cy + s, g.dy - 1);
-  const int z0 = max(cz - s, 0), z1 = min(cz + s, g.dz - 1);
-  uint32_t n = 0;
-  for (int z = z0; z <= z1; ++z)
-    for (int y = y0; y <= y1; ++y) {
-      const uint32_t row = g.cell_base + ((uint32_t)z * (uint32_t)g.dy + (uint32_t)y) * (uint32_t)g.dx;
-      n += __ldg(cells + row + x1 + 1) - __ldg(cells + row + x0);
+// The three box counts N_0..N_2 in one pass over the 25 rows of the 5 x 5 x 5 box: the six
+// offsets a row needs (x - 2 .. x + 3) sit in one or two 32-byte sectors.
+static_assert(kShells == 3, "box_counts3 counts three shells");
+__device__ __forceinline__ void box_counts3(const CloudGrid& g, const uint32_t* cells, int cx,
+                                            int cy, int cz, uint32_t* N) {
+  const int x0 = max(cx - 2, 0), x1 = min(cx + 2, g.dx - 1);
+  const int i0 = max(cx - 1, 0), i1 = min(cx + 1, g.dx - 1);
+  uint32_t n0 = 0, n1 = 0, n2 = 0;
+  for (int dz = -2; dz <= 2; ++dz) {
+    const int z = cz + dz;
+    if (z < 0 || z >= g.dz) continue;
+    for (int dy = -2; dy <= 2; ++dy) {
+      const int y = cy + dy;
+      if (y < 0 || y >= g.dy) continue;
+      const uint32_t* row = cells + g.cell_base + ((uint32_t)z * (uint32_t)g.dy + (uint32_t)y) * (uint32_t)g.dx;
+      n2 += __ldg(row + x1 + 1) - __ldg(row + x0);
+      if (dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
+        n1 += __ldg(row + i1 + 1) - __ldg(row + i0);
+        if (dy == 0 && dz == 0) n0 += __ldg(row + cx + 1) - __ldg(row + cx);
+      }
     }
-  return n;
+  }
+  N[0] = n0;
+  N[1] = n1;
+  N[2] = n2;
 }
 
 __global__ void __launch_bounds__(256)
@@ -86,12 +98,24 @@ k_widths(WidthArgs a) {
   }
   const MlpView mv = mlp_view(s_model);
   const uint32_t total_cells = a.total_cells ? *a.total_cells : 0u;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_queries;
-       i += gridDim.x * blockDim.x) {
+  // queries that are the points are taken in cell order (neighbouring threads read the
+  // same cell rows); only the points placed in cells are there, the rest keep no width
+  // (that happens only when the grid plan failed, which the call reports as an error)
+  const uint32_t n_items = a.spts ? min(a.n_queries, __ldg(a.cells + total_cells)) : a.n_queries;
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items;
+       it += gridDim.x * blockDim.x) {
+    uint32_t i = it;
+    float qx, qy, qz;
+    if (a.spts) {
+      const float4 p = __ldg(a.spts + it);
+      i = __float_as_uint(p.w);
+      if (i >= a.n_queries) continue;
+      qx = p.x; qy = p.y; qz = p.z;
+    } else {
+      qx = __ldg(a.xyz + 3ull * i); qy = __ldg(a.xyz + 3ull * i + 1); qz = __ldg(a.xyz + 3ull * i + 2);
+    }
     const uint32_t cloud = find_cloud(a.t.query_off, a.t.n_clouds, i);
     const CloudGrid g = a.grids[cloud];
-    const float qx = __ldg(a.xyz + 3ull * i), qy = __ldg(a.xyz + 3ull * i + 1),
-                qz = __ldg(a.xyz + 3ull * i + 2);
     if ((uint64_t)g.cell_base + g.n_cells > (uint64_t)total_cells) {  // overran: full radius
       a.qwidth[i] = a.radius;
       continue;
@@ -100,8 +124,7 @@ k_widths(WidthArgs a) {
     const int cy = clamp_cell(cell_coord_f(qy, g.oy, g.inv_cell), g.dy);
     const int cz = clamp_cell(cell_coord_f(qz, g.oz, g.inv_cell), g.dz);
     uint32_t N[kShells];
-#pragma unroll
-    for (int s = 0; s < kShells; ++s) N[s] = box_count(g, a.cells, cx, cy, cz, s);
+    box_counts3(g, a.cells, cx, cy, cz, N);
     // offset of the query from its cell's centre, in cells (0 .. 0.87)
     const float ox = (qx - g.ox) * g.inv_cell - ((float)cx + 0.5f);
     const float oy = (qy - g.oy) * g.inv_cell - ((float)cy + 0.5f);
