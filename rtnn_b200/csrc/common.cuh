@@ -20,8 +20,8 @@ constexpr int kScanItems = 16;      // items per thread of the scan
 constexpr int kScanThreads = 256;
 constexpr int kScanTile = kScanItems * kScanThreads;   // 4096
 constexpr int kRadixThreads = 256;  // 8 warps
-constexpr int kRadixItems = 16;     // per lane, per warp sub-tile of 512
-constexpr int kRadixTile = kRadixThreads * kRadixItems; // 4096 keys per block
+constexpr int kRadixItems = 8;      // per lane, per warp sub-tile of 256
+constexpr int kRadixTile = kRadixThreads * kRadixItems; // 2048 keys per block
 constexpr int kMaxK = 128;
 constexpr int kMaxPasses = 8;       // main search pass + escalating fallback passes
 

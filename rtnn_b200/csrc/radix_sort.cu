@@ -5,8 +5,10 @@
 // in Morton order. Each pass: (1) per-tile digit histograms, column-major
 // [digit][tile]; (2) one exclusive scan of that table (scan.cu), giving every
 // (digit, tile) its global output offset; (3) a stable scatter: each warp ranks its
-// 512-key sub-tile with __match_any_sync, warps are combined through a shared-memory
-// prefix per digit, and keys keep their input order within a digit.
+// sub-tile with __match_any_sync, warps are combined through a shared-memory prefix per
+// digit, the tile is placed in digit order in shared memory, and written out from there
+// so that consecutive threads write consecutive output positions of a digit's run (keys
+// keep their input order within a digit).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -44,7 +46,12 @@ __global__ void __launch_bounds__(kRadixThreads)
 k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 KeyT* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
                 uint32_t shift, const uint32_t* __restrict__ offsets, uint32_t n_tiles) {
-  __shared__ uint32_t s_cnt[kWarps][256];
+  __shared__ uint32_t s_cnt[kWarps][256];   // per warp and digit: count, then tile position
+  __shared__ uint32_t s_start[256];         // per digit: first tile position
+  __shared__ uint32_t s_dst[256];           // per digit: global offset minus s_start
+  __shared__ KeyT s_keys[kRadixTile];       // the tile in digit order
+  __shared__ uint32_t s_vals[kRadixTile];
+  __shared__ uint32_t s_wsum[kRadixThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kWarps * 256; i += blockDim.x) (&s_cnt[0][0])[i] = 0u;
   __syncthreads();
@@ -52,6 +59,7 @@ k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ v
   KeyT k[kRadixItems];
   uint32_t v[kRadixItems], rk[kRadixItems];
   const uint32_t lt = lanemask_lt();
+  // 1. rank every key among the equal digits of its warp, in input order
 #pragma unroll
   for (int it = 0; it < kRadixItems; ++it) {
     const uint32_t i = base + it * 32 + lane;
@@ -68,9 +76,28 @@ k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ v
     __syncwarp();
   }
   __syncthreads();
-  // per digit: global offset of this tile, then the warps in order
-  for (int d = threadIdx.x; d < 256; d += blockDim.x) {
-    uint32_t run = offsets[(uint64_t)d * n_tiles + blockIdx.x];
+  // 2. tile positions: digits in order, warps in order within a digit (stable)
+  static_assert(kRadixThreads == 256, "one thread per digit");
+  {
+    const int d = threadIdx.x;
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) tot += s_cnt[w][d];
+    // exclusive scan of the 256 digit totals: warp scans, then the warp sums
+    uint32_t incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += s_wsum[w];
+    const uint32_t start = before + incl - tot;
+    s_start[d] = start;
+    s_dst[d] = offsets[(uint64_t)d * n_tiles + blockIdx.x] - start;
+    uint32_t run = start;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
       const uint32_t c = s_cnt[w][d];
@@ -79,15 +106,25 @@ k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ v
     }
   }
   __syncthreads();
+  // 3. the tile into shared memory in digit order
 #pragma unroll
   for (int it = 0; it < kRadixItems; ++it) {
     const uint32_t i = base + it * 32 + lane;
     if (i < n) {
       const uint32_t digit = (uint32_t)(k[it] >> shift) & 0xffu;
-      const uint32_t dst = s_cnt[warp][digit] + rk[it];
-      keys_out[dst] = k[it];
-      vals_out[dst] = v[it];
+      const uint32_t li = s_cnt[warp][digit] + rk[it];
+      s_keys[li] = k[it];
+      s_vals[li] = v[it];
     }
+  }
+  __syncthreads();
+  // 4. consecutive tile positions of one digit go to consecutive output positions
+  const uint32_t count = min((uint32_t)kRadixTile, n - blockIdx.x * (uint32_t)kRadixTile);
+  for (uint32_t j = threadIdx.x; j < count; j += blockDim.x) {
+    const KeyT key = s_keys[j];
+    const uint32_t dst = s_dst[(uint32_t)(key >> shift) & 0xffu] + j;
+    keys_out[dst] = key;
+    vals_out[dst] = s_vals[j];
   }
 }
 
