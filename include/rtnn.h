@@ -179,6 +179,10 @@ typedef struct rtnn_tuning {
                                  2: tiles for the first pass, one warp per query for the
                                  escalation passes (scattered short queries). K <= 64 for
                                  the per-query kernel; larger K always use the tiles */
+  float buckets_per_halving;  /* partitioned search: density buckets (sort-key levels) per
+                                 halving of the search width (0..8; 0: all narrowed widths
+                                 in one bucket). Fewer buckets keep tiles spatially tighter,
+                                 more keep a tile's widths alike */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

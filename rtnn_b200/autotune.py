@@ -41,6 +41,7 @@ GRID_PRESETS = [
     {"cell_ratio": 1.0, "min_cell_ratio": 0.0625, "points_per_cell": 4.0, "query_warps": 0},
 ]
 LEARNED_KNOBS = [
+    ("buckets_per_halving", [0.0, 0.5, 1.0, 2.0]),
     ("width_margin", [1.0, 1.08, 1.15, 1.25, 1.4]),
     ("fallback_passes", [2, 4, 6]),
 ]

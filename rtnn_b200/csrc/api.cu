@@ -101,7 +101,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f, 16u, 0u};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f, 16u, 0u, 1.0f};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
@@ -360,7 +360,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   const bool key64 = key64_of(sh, pr);
   RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.morton_bits,
                             part ? (const float*)ws.qwidth_in.p : nullptr, pr.radius,
-                            level_bits_of(pr), key64, ws.keys0.p, s),
+                            level_bits_of(pr), tu.buckets_per_halving, key64, ws.keys0.p, s),
           "query keys");
   bool in1 = false;
   RTNN_CU(radix_sort_pairs(key64, ws.keys0.p, (uint32_t*)ws.vals0.p, ws.keys1.p,
@@ -622,7 +622,8 @@ rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
       !(t->points_per_cell >= 0.f) || t->fallback_passes > kMaxPasses - 2 ||
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f) ||
       !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f) || t->pending_slots < 8 ||
-      t->pending_slots > 256 || t->query_warps > 2)
+      t->pending_slots > 256 || t->query_warps > 2 ||
+      !(t->buckets_per_halving >= 0.f && t->buckets_per_halving <= 8.f))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
   return RTNN_OK;

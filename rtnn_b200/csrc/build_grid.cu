@@ -272,11 +272,13 @@ k_scatter(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cl
   }
 }
 
-// Density bucket of a width: 0 for the full radius, then two buckets per halving.
-__device__ __forceinline__ uint32_t width_level(float w, float radius, uint32_t level_bits) {
+// Density bucket of a width: 0 for the full radius, then `per_halving` buckets for each
+// halving of the width (0: one bucket for every narrowed width).
+__device__ __forceinline__ uint32_t width_level(float w, float radius, uint32_t level_bits,
+                                                float per_halving) {
   if (!(w < radius)) return 0u;
   const uint32_t top = (1u << level_bits) - 1u;
-  const float l = ceilf(-2.f * log2f(fmaxf(w, 1e-30f) / radius));
+  const float l = ceilf(-per_halving * log2f(fmaxf(w, 1e-30f) / radius));
   return (uint32_t)fminf(fmaxf(l, 1.f), (float)top);
 }
 
@@ -286,7 +288,7 @@ __global__ void __launch_bounds__(256)
 k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
              CloudTables t, const CloudGrid* __restrict__ grids, uint32_t morton_bits,
              const float* __restrict__ qwidth, float radius, uint32_t level_bits,
-             KeyT* __restrict__ keys) {
+             float per_halving, KeyT* __restrict__ keys) {
   __shared__ float s_xyz[kChunk * 3];
   const ChunkRange r = chunk_range(t.qchunk_base, t.query_off, t.n_clouds, blockIdx.x);
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
@@ -297,7 +299,7 @@ k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
     const int fy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.morton_scale), top + 1);
     const int fz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.morton_scale), top + 1);
     const uint64_t m = morton3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz);
-    const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits) : 0u;
+    const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits, per_halving) : 0u;
     keys[r.begin + i] = ((KeyT)r.cloud << (3 * morton_bits + level_bits)) |
                         ((KeyT)lvl << (3 * morton_bits)) | (KeyT)m;
   }
@@ -378,16 +380,17 @@ cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
 cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
                               const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
                               uint32_t morton_bits, const float* qwidth, float radius,
-                              uint32_t level_bits, bool key64, void* keys, cudaStream_t s) {
+                              uint32_t level_bits, float per_halving, bool key64, void* keys,
+                              cudaStream_t s) {
   if (n_qchunks == 0) return cudaSuccess;
   if (key64)
     k_query_keys<uint64_t><<<n_qchunks, 256, 0, s>>>(xyz, 3 * n_queries, aligned, t, grids,
                                                      morton_bits, qwidth, radius, level_bits,
-                                                     (uint64_t*)keys);
+                                                     per_halving, (uint64_t*)keys);
   else
     k_query_keys<uint32_t><<<n_qchunks, 256, 0, s>>>(xyz, 3 * n_queries, aligned, t, grids,
                                                      morton_bits, qwidth, radius, level_bits,
-                                                     (uint32_t*)keys);
+                                                     per_halving, (uint32_t*)keys);
   return cudaGetLastError();
 }
 

@@ -80,7 +80,8 @@ cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
 cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
                               const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
                               uint32_t morton_bits, const float* qwidth, float radius,
-                              uint32_t level_bits, bool key64, void* keys, cudaStream_t s);
+                              uint32_t level_bits, float per_halving, bool key64, void* keys,
+                              cudaStream_t s);
 cudaError_t launch_gather_queries(const float* xyz, const uint32_t* order, uint32_t n,
                                   float4* sq, const float* w_in, float* w_out, int n_sms,
                                   cudaStream_t s);

@@ -164,7 +164,8 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
     e = launch_scan_excl(cells, 0, &ctr->total_cells, 1, cap + 1, scan_state, &ctr->scan_tiles[0], ctr, s);
   if (e == cudaSuccess) e = launch_scatter(d_points, N, ap, t, n_chunks, grids, cells, rank, spts, ctr, s);
   if (e == cudaSuccess)
-    e = launch_query_keys(d_qs, Q, aq, t, n_qchunks, grids, mb, nullptr, radius, 0, false, keys0, s);
+    e = launch_query_keys(d_qs, Q, aq, t, n_qchunks, grids, mb, nullptr, radius, 0, 0.f, false,
+                          keys0, s);
   if (e == cudaSuccess)
     e = radix_sort_pairs(false, keys0, vals0, keys1, vals1, (uint32_t)Q, key_bits, true, hist,
                          scan_state, &ctr->scan_tiles[1], ctr, &in1, s);
