@@ -109,6 +109,11 @@ struct rtnn_ctx {
   DevBuf model;
   bool has_model = false;
   DevBuf train_grad, train_m, train_v, train_loss;
+  // host-buffer batches in sub-batches (run_batched_overlapped): download stream, per
+  // sub-batch stage events, per sub-batch counters
+  cudaStream_t copy = nullptr;
+  cudaEvent_t sub_ev[8][5] = {};
+  DevBuf sub_ctr;
 };
 
 struct rtnn_plan {
@@ -305,7 +310,8 @@ uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats) {
 
 rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr,
                   const float* d_pts, const float* d_qs, int32_t* d_out, cudaStream_t s,
-                  cudaEvent_t* ev, float* feats_out = nullptr, float* cellsz_out = nullptr) {
+                  cudaEvent_t* ev, float* feats_out = nullptr, float* cellsz_out = nullptr,
+                  uint32_t index_base = 0) {
   Counters* ctr = (Counters*)ws.counters.p;
   const bool knn = pr.mode == RTNN_MODE_KNN;
   const rtnn_tuning& tu = c->tuning;
@@ -388,6 +394,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.radius = pr.radius;
   a.r2 = pr.radius * pr.radius;
   a.k = pr.k;
+  a.index_base = index_base;
   a.lane_walk_ratio = tu.lane_walk_ratio;
   a.gap_ratio = tu.gap_ratio;
   a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
@@ -547,6 +554,145 @@ rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const fl
   return read_back(c, c->ws, s, sh, pr, stats, true);
 }
 
+// Host buffers, many clouds: the batch runs as sub-batches of whole clouds (about equal
+// query counts) on the context's stream, and a second stream downloads each sub-batch's
+// rows as soon as it is done -- the rows of consecutive clouds are contiguous and clouds
+// are independent -- so the result download (4 K bytes per query) overlaps the search of
+// the sub-batches after it. Every sub-batch is enqueued before any download, so the host
+// never waits on a download while work is still to be issued (a download into pageable
+// memory returns only once done). Same rows as one batch; stats are summed.
+constexpr uint32_t kMaxSub = 8;
+constexpr uint64_t kOverlapMinBytes = 256ull << 20;   // smaller outputs: one batch
+
+uint32_t overlap_sub_batches(uint64_t out_bytes, uint32_t n_clouds) {
+  if (out_bytes < kOverlapMinBytes || n_clouds < 2) return 1;
+  return (uint32_t)std::min<uint64_t>({kMaxSub, n_clouds, std::max<uint64_t>(2, out_bytes / (256ull << 20))});
+}
+
+rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_clouds,
+                                   const float* points, const float* queries,
+                                   const uint64_t* query_off, const Params& pr, int32_t* out,
+                                   rtnn_stats* stats, uint32_t n_sub) {
+  const uint64_t* qoff = queries ? query_off : point_off;
+  const uint64_t N = point_off[n_clouds], Q = qoff[n_clouds];
+  // cloud boundaries: sub-batch g starts at the first cloud holding query Q * g / n_sub
+  std::vector<uint32_t> cut{0};
+  for (uint32_t g = 1; g < n_sub; ++g) {
+    const uint64_t target = Q * g / n_sub;
+    uint32_t ci = (uint32_t)(std::upper_bound(qoff, qoff + n_clouds + 1, target) - qoff);
+    ci = std::min(ci, n_clouds);
+    if (ci > cut.back() && ci < n_clouds) cut.push_back(ci);
+  }
+  cut.push_back(n_clouds);
+  const uint32_t G = (uint32_t)cut.size() - 1;
+  std::vector<Shapes> shs(G);
+  std::vector<uint64_t> po, qo;
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint32_t c0 = cut[g], nc = cut[g + 1] - cut[g];
+    po.assign(point_off + c0, point_off + c0 + nc + 1);
+    for (auto& v : po) v -= point_off[c0];
+    if (queries) {
+      qo.assign(query_off + c0, query_off + c0 + nc + 1);
+      for (auto& v : qo) v -= query_off[c0];
+    }
+    rtnn_status st = batched_shapes(c, po.data(), nc, queries ? qo.data() : nullptr, c->tuning, shs[g]);
+    if (st != RTNN_OK) return st;
+    st = reserve(c, c->ws, shs[g], pr);   // grows the workspace to the largest sub-batch
+    if (st != RTNN_OK) return st;
+  }
+  cudaStream_t s = stream_of(c);
+  if (!c->copy) RTNN_CU(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking), "create stream");
+  for (auto& row : c->sub_ev)
+    for (auto& e : row)
+      if (!e) RTNN_CU(cudaEventCreate(&e), "create event");
+  const size_t out_bytes = (size_t)Q * pr.k * sizeof(int32_t);
+  RTNN_CU(ensure(c->ws.in_pts, std::max<uint64_t>(N, 1) * 12), "alloc points");
+  RTNN_CU(ensure(c->ws.out, out_bytes), "alloc output");
+  RTNN_CU(ensure(c->sub_ctr, (size_t)kMaxSub * sizeof(Counters)), "alloc counters");
+  RTNN_CU(cudaMemcpyAsync(c->ws.in_pts.p, points, N * 12, cudaMemcpyHostToDevice, s), "copy points");
+  const float* d_pts = (const float*)c->ws.in_pts.p;
+  const float* d_qs = d_pts;
+  if (queries) {
+    RTNN_CU(ensure(c->ws.in_qs, Q * 12), "alloc queries");
+    RTNN_CU(cudaMemcpyAsync(c->ws.in_qs.p, queries, Q * 12, cudaMemcpyHostToDevice, s), "copy queries");
+    d_qs = (const float*)c->ws.in_qs.p;
+  }
+  int32_t* d_out = (int32_t*)c->ws.out.p;
+  Counters* d_sub = (Counters*)c->sub_ctr.p;
+  for (uint32_t g = 0; g < G; ++g) {
+    const Shapes& sh = shs[g];
+    RTNN_CU(cudaMemcpyAsync(c->ws.tables.p, sh.tab.data(), sh.tab.size() * 4, cudaMemcpyHostToDevice, s),
+            "copy tables");
+    if (sh.N == 0) {
+      RTNN_CU(cudaMemsetAsync(d_out + qoff[cut[g]] * pr.k, 0xff, sh.Q * pr.k * 4, s), "fill output");
+      RTNN_CU(cudaMemsetAsync(d_sub + g, 0, sizeof(Counters), s), "clear counters");
+      for (int i = 0; i < 5; ++i) RTNN_CU(cudaEventRecord(c->sub_ev[g][i], s), "event");
+    } else {
+      const rtnn_status st = issue(c, c->ws, sh, pr, d_pts + 3 * point_off[cut[g]],
+                                   d_qs + 3 * qoff[cut[g]], d_out + qoff[cut[g]] * pr.k, s,
+                                   c->sub_ev[g], nullptr, nullptr, (uint32_t)point_off[cut[g]]);
+      if (st != RTNN_OK) return st;
+      RTNN_CU(cudaMemcpyAsync(d_sub + g, c->ws.counters.p, sizeof(Counters), cudaMemcpyDeviceToDevice, s),
+              "save counters");
+    }
+  }
+  for (uint32_t g = 0; g < G; ++g) {   // each download after its sub-batch's last event
+    RTNN_CU(cudaStreamWaitEvent(c->copy, c->sub_ev[g][4], 0), "wait");
+    const uint64_t q0 = qoff[cut[g]], nq = qoff[cut[g + 1]] - q0;
+    if (nq)
+      RTNN_CU(cudaMemcpyAsync(out + q0 * pr.k, d_out + q0 * pr.k, nq * pr.k * 4, cudaMemcpyDeviceToHost,
+                              c->copy),
+              "copy output");
+  }
+  RTNN_CU(cudaStreamSynchronize(c->copy), "synchronize");
+  std::vector<Counters> h(G);
+  RTNN_CU(cudaMemcpyAsync(h.data(), d_sub, G * sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
+  RTNN_CU(cudaMemcpyAsync(c->h_grid, c->ws.grids.p, sizeof(CloudGrid), cudaMemcpyDeviceToHost, s), "read grid");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  for (uint32_t g = 0; g < G; ++g) {
+    const Counters& hc = h[g];
+    if (hc.error == kErrScanTimeout)
+      return fail(c, RTNN_ERR_DEVICE_TIMEOUT, "scan look-back gave up waiting on tile " + std::to_string(hc.error_info));
+    if (hc.error == kErrCellCapacity)
+      return fail(c, RTNN_ERR_INTERNAL, "grid plan exceeded its cell capacity (cloud " + std::to_string(cut[g] + hc.error_info) + ")");
+    if (hc.error != 0) return fail(c, RTNN_ERR_INTERNAL, "device error " + std::to_string(hc.error));
+  }
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->n_points = N;
+    stats->n_queries = Q;
+    stats->n_clouds = n_clouds;
+    stats->n_buckets = partitioned(pr) ? 2 : 1;
+    stats->cell_size = c->h_grid->cell;
+    stats->grid_dims[0] = (uint32_t)c->h_grid->dx;
+    stats->grid_dims[1] = (uint32_t)c->h_grid->dy;
+    stats->grid_dims[2] = (uint32_t)c->h_grid->dz;
+    for (uint32_t g = 0; g < G; ++g) {
+      const Shapes& sh = shs[g];
+      if (partitioned(pr)) stats->n_fallback += h[g].fb_count[0];
+      stats->n_tiles += sh.n_tiles;
+      stats->n_cells += h[g].total_cells;
+      stats->n_launches += sh.N ? launches_of(sh, pr, false) : 0;
+      stats->n_loaded += h[g].n_loaded;
+      stats->n_tested += h[g].n_tested;
+      float t[5] = {0, 0, 0, 0, 0};
+      if (sh.N) {
+        cudaEventElapsedTime(&t[0], c->sub_ev[g][0], c->sub_ev[g][1]);
+        cudaEventElapsedTime(&t[1], c->sub_ev[g][1], c->sub_ev[g][2]);
+        cudaEventElapsedTime(&t[2], c->sub_ev[g][2], c->sub_ev[g][4]);
+        cudaEventElapsedTime(&t[3], c->sub_ev[g][3], c->sub_ev[g][4]);
+        cudaEventElapsedTime(&t[4], c->sub_ev[g][0], c->sub_ev[g][4]);
+      }
+      stats->ms_build += t[0];
+      stats->ms_partition += t[1];
+      stats->ms_search += t[2];
+      stats->ms_fallback += t[3];
+      stats->ms_total += t[4];
+    }
+  }
+  return RTNN_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -594,6 +740,11 @@ rtnn_status rtnn_destroy(rtnn_ctx* c) {
   release(c->train_loss);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& row : c->sub_ev)
+    for (auto& e : row)
+      if (e) cudaEventDestroy(e);
+  release(c->sub_ctr);
+  if (c->copy) cudaStreamDestroy(c->copy);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
   if (c->h_grid) cudaFreeHost(c->h_grid);
   if (c->own) cudaStreamDestroy(c->own);
@@ -669,6 +820,11 @@ rtnn_status rtnn_search_batched(rtnn_ctx* c, const float* points, const uint64_t
   const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
   st = reserve(c, c->ws, sh, pr);
   if (st != RTNN_OK) return st;
+  const uint32_t n_sub = (flags & RTNN_FLAG_DEVICE_POINTERS) || sh.N == 0
+                            ? 1u : overlap_sub_batches((uint64_t)sh.Q * k * 4, n_clouds);
+  if (n_sub > 1)
+    return run_batched_overlapped(c, point_offsets, n_clouds, points, queries, query_offsets, pr,
+                                  out, stats, n_sub);
   cudaStream_t s = stream_of(c);
   RTNN_CU(cudaMemcpyAsync(c->ws.tables.p, sh.tab.data(), sh.tab.size() * 4, cudaMemcpyHostToDevice, s),
           "copy tables");

@@ -38,6 +38,8 @@ struct SearchArgs {
   uint32_t pending;            // appended-hit slots per lane beyond the k kept ones
   uint32_t qcap;               // k_search_q: hit buffer entries per warp (search_q_cap)
   uint32_t flags;              // kSearch*
+  uint32_t index_base;         // added to every point index written (0 unless the points
+                               // passed are a part of the caller's array)
   int pass;                    // kPassMain, kPassEscalate or kPassFinal
   float lane_walk_ratio;       // tile spread > ratio * width: per-lane walk (0: never)
   float gap_ratio;             // split a tile where consecutive queries are farther apart

@@ -499,7 +499,8 @@ k_search(SearchArgs a) {
       }
       __syncwarp();
       // 5. coalesced row writes
-      const uint32_t sub = local_idx ? a.t.point_off[gcloud] : 0u;
+      // row entries: index within the cloud (local) or + index_base (a part of a batch)
+      const uint32_t sub = local_idx ? a.t.point_off[gcloud] : 0u - a.index_base;
       uint32_t wm = __ballot_sync(0xffffffffu, done);
       while (wm) {
         const int L = __ffs(wm) - 1;
@@ -775,7 +776,7 @@ k_search_q(SearchArgs a) {
         warp_select(buf, nb, found);
       }
       __syncwarp();
-      const uint32_t sub = local_idx ? a.t.point_off[cj] : 0u;
+      const uint32_t sub = local_idx ? a.t.point_off[cj] : 0u - a.index_base;
       for (uint32_t jj = lane; jj < k; jj += 32)
         row[jj] = jj < found ? (int32_t)((uint32_t)buf[jj] - sub) : -1;
       __syncwarp();

@@ -236,6 +236,26 @@ def test_batched_matches_per_cloud_oracle(ctx):
         assert st.n_clouds == 64
 
 
+def test_batched_host_buffers_in_sub_batches(ctx):
+    """A host-buffer batch whose rows exceed 256 MB runs as sub-batches of whole clouds with
+    the downloads overlapped: same rows as the device-pointer call (one batch), stats summed."""
+    import torch
+    p, off = wl.multicloud(n_clouds=64, lo=8000, hi=40000, seed=21)
+    k = 64
+    assert p.shape[0] * k * 4 >= 256 << 20
+    tp = torch.from_numpy(p).cuda()
+    for kw in ({}, {"partition": True}):
+        dev = ctx.search_batched(tp, off, mode="knn", radius=0.2, k=k, sorted_rows=True, **kw)
+        st = rtnn_b200.Stats()
+        host = ctx.search_batched(p, off, mode="knn", radius=0.2, k=k, sorted_rows=True, stats=st,
+                                  **kw)
+        assert np.array_equal(host, dev.cpu().numpy())
+        assert st.n_queries == p.shape[0] and st.n_clouds == 64 and st.ms_total > 0
+    anyk = ctx.search_batched(p, off, mode="radius", radius=0.2, k=k, any_k=True)
+    full = ctx.search_batched(tp, off, mode="radius", radius=0.2, k=k).cpu().numpy()
+    assert np.array_equal((anyk >= 0).sum(1), (full >= 0).sum(1))
+
+
 def test_batched_separate_queries_and_empty_clouds(ctx):
     rng = np.random.default_rng(8)
     psz = [100, 0, 50, 300, 1]
