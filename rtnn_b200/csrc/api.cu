@@ -3,7 +3,7 @@
 // The pipeline replaces the timed region of optixNSearch (src/optixNSearch/main.cpp:91-148):
 //   uploadData/computeMinMax (optix.cpp:117-168)      -> k_bbox, k_grid_plan
 //   sortParticles/gridSort (sort.cpp:500-692)         -> k_count, scan, k_scatter
-//   query Morton order + partition (sort.cpp:393-498) -> k_query_keys, radix sort, k_widths
+//   query Hilbert order + partition (sort.cpp:393-498) -> k_query_keys, radix sort, k_widths
 //   createGeometry/gasSortSearch/search (search.cpp)  -> k_search (+ fallback pass)
 // Every step is issued on one stream with no host synchronisation, so the same code
 // path is captured into a CUDA graph by rtnn_plan_execute. Sizes that are only known on
@@ -164,7 +164,7 @@ rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32
 }
 
 void finish_shapes(Shapes& sh, const rtnn_tuning& tu) {
-  // Morton steps per axis: about 64 key cells per query of the largest cloud
+  // Hilbert steps per axis: about 64 key cells per query of the largest cloud
   uint32_t mb = (ceil_log2(std::max<uint64_t>(sh.max_cloud_q, 2)) + 6 + 2) / 3;
   mb = std::max(1u, std::min(16u, mb));
   const uint32_t cb = ceil_log2(sh.n_clouds);
@@ -340,7 +340,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   if (ev) RTNN_CU(cudaEventRecord(ev[1], s), "event");
 
   // density buckets: a width per query (caller's order), then the sort key
-  // cloud | bucket of the width | Morton code, so each 32-query tile shares one width
+  // cloud | bucket of the width | Hilbert index, so each 32-query tile shares one width
   const bool part = partitioned(pr);
   if (part || feats_out) {
     WidthArgs w{};
@@ -422,7 +422,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   // order-preserving compaction (scan of the flags) turns them into list p%2 at a wider
   // width (grown by the density each query saw, at most doubled), and escalation pass p
   // reads list (p-1)%2; the final pass searches what
-  // is left at the full radius. Lists stay in (cloud, bucket, Morton) order, so fallback
+  // is left at the full radius. Lists stay in (cloud, bucket, Hilbert) order, so fallback
   // tiles remain spatially coherent.
   const int n_fb = part ? (int)fallback_passes_of(pr) : 0;
   uint32_t* flags = (uint32_t*)ws.fbflag.p;

@@ -175,7 +175,7 @@ k_grid_plan(CloudTables t, const uint32_t* __restrict__ bbox, float radius, floa
       g.cell = cell; g.inv_cell = 1.0f / cell;
       g.dx = d[0]; g.dy = d[1]; g.dz = d[2];
       g.n_cells = (uint32_t)((uint64_t)d[0] * d[1] * d[2]);
-      // query order: Morton code on 2^morton_bits steps across the cloud's longest side
+      // query order: Hilbert index on 2^morton_bits steps across the cloud's longest side
       // (finer than the cells, so dense cells still yield compact 32-query tiles)
       const float ext = fmaxf(fmaxf(mx[0] - mn[0], mx[1] - mn[1]), fmaxf(mx[2] - mn[2], 1e-30f));
       g.morton_scale = (float)((1u << morton_bits) - 1u) / ext;
@@ -282,7 +282,7 @@ __device__ __forceinline__ uint32_t width_level(float w, float radius, uint32_t 
   return (uint32_t)fminf(fmaxf(l, 1.f), (float)top);
 }
 
-// Sort key per query: cloud | density bucket of its width | Morton code of its cell.
+// Sort key per query: cloud | density bucket of its width | Hilbert index of its cell.
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
 k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
@@ -298,7 +298,7 @@ k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
     const int fx = clamp_cell(cell_coord_f(s_xyz[3 * i], g.ox, g.morton_scale), top + 1);
     const int fy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.morton_scale), top + 1);
     const int fz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.morton_scale), top + 1);
-    const uint64_t m = morton3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz);
+    const uint64_t m = hilbert3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz, morton_bits);
     const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits, per_halving) : 0u;
     keys[r.begin + i] = ((KeyT)r.cloud << (3 * morton_bits + level_bits)) |
                         ((KeyT)lvl << (3 * morton_bits)) | (KeyT)m;

@@ -143,6 +143,41 @@ __device__ __forceinline__ uint64_t morton3_64(uint32_t x, uint32_t y, uint32_t 
   return spread3_64(x) | (spread3_64(y) << 1) | (spread3_64(z) << 2);
 }
 
+// Hilbert index of a cell (b bits per axis), after J. Skilling, "Programming the Hilbert
+// curve" (AIP Conf. Proc. 707, 2004): the axes are turned into the curve's transposed
+// form (undo the excess work: invert or exchange low bits, top bit down; then Gray-encode),
+// and the transposed words interleave bit by bit, the first word most significant.
+// Consecutive indices are face-adjacent cells, so a run of consecutive queries stays
+// compact where the Morton order jumps.
+__device__ __forceinline__ uint64_t hilbert3_64(uint32_t x, uint32_t y, uint32_t z, uint32_t b) {
+  uint32_t X0 = x, X1 = y, X2 = z;
+  const uint32_t M = 1u << (b - 1);
+  for (uint32_t Q = M; Q > 1; Q >>= 1) {
+    const uint32_t P = Q - 1;
+    if (X0 & Q) X0 ^= P;
+    if (X1 & Q) {
+      X0 ^= P;
+    } else {
+      const uint32_t t = (X0 ^ X1) & P;
+      X0 ^= t;
+      X1 ^= t;
+    }
+    if (X2 & Q) {
+      X0 ^= P;
+    } else {
+      const uint32_t t = (X0 ^ X2) & P;
+      X0 ^= t;
+      X2 ^= t;
+    }
+  }
+  X1 ^= X0;
+  X2 ^= X1;
+  uint32_t t = 0;
+  for (uint32_t Q = M; Q > 1; Q >>= 1)
+    if (X2 & Q) t ^= Q - 1;
+  return morton3_64(X2 ^ t, X1 ^ t, X0 ^ t);
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m;
 }

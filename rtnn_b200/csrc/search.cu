@@ -5,7 +5,7 @@
 // programs __intersection__sphere_radius / __intersection__sphere_knn with
 // check_intersect, write_res_radius and insertTopKQ (geometry.cu:38-191).
 //
-// Work item = a tile of 32 Morton-ordered queries of one cloud, handled by one warp;
+// Work item = a tile of 32 Hilbert-ordered queries of one cloud, handled by one warp;
 // a persistent grid pulls tiles from an atomic counter. Per tile:
 //   1. the warp reduces the tiles's bounding box and widest search width R;
 //   2. the candidate cells are the grid box covering bbox +- R; in raster order each
@@ -235,8 +235,8 @@ k_search(SearchArgs a) {
     bool short_lane = false;   // narrowed search that found fewer than K neighbors
     // The tile is searched as runs of consecutive queries: a run ends where the next query
     // (in sort order) belongs to another cloud or lies farther than gap_ratio x the widest
-    // width from its predecessor, so a jump of the Morton curve never stretches one
-    // candidate box over the space between two distant groups.
+    // width from its predecessor, so a jump of the curve (between clouds, buckets or sparse
+    // regions) never stretches one candidate box over the space between two distant groups.
     const float gap = a.gap_ratio * wmax(valid ? w : 0.f);
     const float prx = __shfl_up_sync(0xffffffffu, q.x, 1);
     const float pry = __shfl_up_sync(0xffffffffu, q.y, 1);
