@@ -38,8 +38,41 @@ __device__ __forceinline__ MlpView mlp_view(const float* P) {
   return v;
 }
 
-// normalised output o (before out_mean/out_std) of one sample
-__device__ __forceinline__ float mlp_forward_norm(const MlpView& m, const float* x) {
+// ---- inference: normalised output o (before out_mean/out_std) of one sample. The second
+// layer uses packed FP32x2 FMAs (sm_100a): two hidden units per instruction, each element
+// rounded like fmaf, accumulated over the inputs in order, so the result is the bits of the
+// plain one-unit-at-a-time loop. W2p holds W2 with the rows of units 2m and 2m + 1
+// interleaved ({W2[2m][i], W2[2m+1][i]} at W2p[m * 2 * kHidden + 2 i]), one 8-byte load per
+// pair.
+__device__ __forceinline__ uint64_t f2pack(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2unpack(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+static_assert(kHidden % 2 == 0, "hidden units are paired");
+
+// Block-wide: the parameters into shared memory, plus W2 with unit pairs interleaved.
+__device__ __forceinline__ void load_model_smem(const float* P, float* s_p, float* s_w2p) {
+  for (int i = threadIdx.x; i < kModelParams; i += blockDim.x) s_p[i] = P[i];
+  __syncthreads();
+  const float* W2 = mlp_view(s_p).W2;
+  for (int e = threadIdx.x; e < kHidden * kHidden; e += blockDim.x) {
+    const int j = e / kHidden, i = e % kHidden;   // W2[j][i]
+    s_w2p[(j >> 1) * 2 * kHidden + 2 * i + (j & 1)] = W2[e];
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ float mlp_forward_norm_x2(const MlpView& m, const float* W2p,
+                                                     const float* x) {
   float xn[kFeatDim];
 #pragma unroll
   for (int f = 0; f < kFeatDim; ++f) xn[f] = (x[f] - m.in_mean[f]) / m.in_std[f];
@@ -53,11 +86,15 @@ __device__ __forceinline__ float mlp_forward_norm(const MlpView& m, const float*
   }
   float o = m.b3;
 #pragma unroll 1
-  for (int j = 0; j < kHidden; ++j) {
-    float s = m.b2[j];
+  for (int j = 0; j < kHidden; j += 2) {
+    uint64_t acc = f2pack(m.b2[j], m.b2[j + 1]);
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(W2p + j * kHidden);
 #pragma unroll
-    for (int i = 0; i < kHidden; ++i) s = fmaf(m.W2[j * kHidden + i], h1[i], s);
-    o = fmaf(m.W3[j], fmaxf(s, 0.f), o);
+    for (int i = 0; i < kHidden; ++i) acc = fma2(w[i], f2pack(h1[i], h1[i]), acc);
+    float s0, s1;
+    f2unpack(acc, s0, s1);
+    o = fmaf(m.W3[j], fmaxf(s0, 0.f), o);
+    o = fmaf(m.W3[j + 1], fmaxf(s1, 0.f), o);
   }
   return o;
 }
@@ -92,10 +129,8 @@ __device__ __forceinline__ void box_counts3(const CloudGrid& g, const uint32_t* 
 __global__ void __launch_bounds__(256)
 k_widths(WidthArgs a) {
   __shared__ float s_model[kModelParams];
-  if (a.model) {
-    for (int i = threadIdx.x; i < kModelParams; i += blockDim.x) s_model[i] = a.model[i];
-    __syncthreads();
-  }
+  __shared__ __align__(8) float s_w2p[kHidden * kHidden];   // W2, unit pairs interleaved
+  if (a.model) load_model_smem(a.model, s_model, s_w2p);
   const MlpView mv = mlp_view(s_model);
   const uint32_t total_cells = a.total_cells ? *a.total_cells : 0u;
   // queries that are the points are taken in cell order (neighbouring threads read the
@@ -138,7 +173,7 @@ k_widths(WidthArgs a) {
     feat[5] = fminf(sqrtf(ox * ox + oy * oy + oz * oz), 1.f);
     float w;
     if (a.model) {
-      const float o = mlp_forward_norm(mv, feat);
+      const float o = mlp_forward_norm_x2(mv, s_w2p, feat);
       const float y = fmaf(o, mv.out_std, mv.out_mean);
       w = a.margin * g.cell * expf(fminf(y, 30.f));
     } else {
@@ -273,14 +308,14 @@ __global__ void __launch_bounds__(256)
 k_mlp_forward(const float* __restrict__ P, const float* __restrict__ feats, uint32_t n,
               float* __restrict__ y) {
   __shared__ float s_p[kModelParams];
-  for (int i = threadIdx.x; i < kModelParams; i += blockDim.x) s_p[i] = P[i];
-  __syncthreads();
+  __shared__ __align__(8) float s_w2p[kHidden * kHidden];
+  load_model_smem(P, s_p, s_w2p);
   const MlpView m = mlp_view(s_p);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float x[kFeatDim];
 #pragma unroll
     for (int f = 0; f < kFeatDim; ++f) x[f] = feats[(size_t)i * kFeatDim + f];
-    y[i] = fmaf(mlp_forward_norm(m, x), m.out_std, m.out_mean);
+    y[i] = fmaf(mlp_forward_norm_x2(m, s_w2p, x), m.out_std, m.out_mean);
   }
 }
 
