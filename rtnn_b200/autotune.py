@@ -21,8 +21,8 @@ import rtnn_b200
 
 # knobs that change the grid (and so the learned model's input features)
 CELL_KNOBS = [
-    ("points_per_cell", [0.0, 0.25, 1.0, 4.0, 16.0]),
-    ("cell_ratio", [0.25, 0.5, 1.0]),
+    ("points_per_cell", [0.0, 0.125, 0.25, 1.0, 4.0, 16.0]),
+    ("cell_ratio", [0.125, 0.25, 0.5, 1.0]),
 ]
 # knobs of the search kernels only
 SEARCH_KNOBS = [
@@ -38,6 +38,7 @@ GRID_KNOBS = CELL_KNOBS + SEARCH_KNOBS
 GRID_PRESETS = [
     {"cell_ratio": 0.5, "min_cell_ratio": 0.0625, "points_per_cell": 1.0, "query_warps": 0},
     {"cell_ratio": 0.25, "min_cell_ratio": 0.02, "points_per_cell": 0.25, "query_warps": 2},
+    {"cell_ratio": 0.125, "min_cell_ratio": 0.01, "points_per_cell": 0.125, "query_warps": 2},
     {"cell_ratio": 1.0, "min_cell_ratio": 0.0625, "points_per_cell": 4.0, "query_warps": 0},
 ]
 LEARNED_KNOBS = [
