@@ -35,9 +35,9 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per query of the main search pass, from the ncu capture in
-# profiles/k_search_knn_multicloud_scale0.1.md (940 MB for 5.25 M queries), scaled by
+# profiles/k_search_knn_multicloud_scale0.1.md (1,102 MB for 5.25 M queries), scaled by
 # queries to a full launch; only known for the default workload.
-TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 179.0}
+TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 210.0}
 
 
 def parse():
@@ -68,7 +68,7 @@ def run_profile(args):
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     # the tuning the autotuner settles on for the default workload: fine cells, tiles for
     # the first pass and one warp per query for the escalation passes
-    ctx.set_tuning(points_per_cell=0.25, cell_ratio=0.25, min_cell_ratio=0.02, width_margin=1.1,
+    ctx.set_tuning(points_per_cell=0.125, cell_ratio=0.125, min_cell_ratio=0.01, width_margin=1.1,
                    fallback_passes=2, gap_ratio=2.0, pending_slots=16, query_warps=2,
                    buckets_per_halving=1.0)
     train_model(ctx, cfg, args.scale, 0)
