@@ -101,7 +101,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.25f, 4u, 0.0f, 2.0f, 16u, 0u, 1.0f};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.1f, 4u, 0.0f, 2.0f, 16u, 2u, 1.0f};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
