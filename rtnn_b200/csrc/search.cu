@@ -7,21 +7,24 @@
 //
 // Work item = a tile of 32 Hilbert-ordered queries of one cloud, handled by one warp;
 // a persistent grid pulls tiles from an atomic counter. Per tile:
-//   1. the warp reduces the tiles's bounding box and widest search width R;
+//   1. the warp reduces the tile's bounding box and widest search width R (per run of
+//      nearby queries, see below);
 //   2. the candidate cells are the grid box covering bbox +- R; in raster order each
 //      (y, z) row of that box is one contiguous range of the cell-sorted points, so a
 //      row costs two offset loads (computed lane-parallel, 32 rows at a time);
-//   3. each range is streamed 32 points at a time with 16-byte loads, the points farther
-//      than R from the tile box are dropped, and the survivors are compacted with
-//      __ballot_sync into a per-warp shared-memory stage;
+//   3. 32 rows at a time are streamed as one flattened candidate sequence with 16-byte
+//      loads (rows in a stride-permuted order), the points farther than R from the tile
+//      box are dropped, and the survivors are compacted with __ballot_sync into a
+//      per-warp shared-memory stage;
 //   4. every lane tests every staged point against its own query with the reference's
 //      FP32 distance (common.cuh: dist2_ref) and keeps its K smallest (distance, index)
 //      pairs in a per-lane column in shared memory ([slot][lane], conflict-free): hits are
 //      appended branch-free and merged into a max-heap of the K kept when a column fills;
 //   5. rows are written warp-cooperatively (coalesced), unused slots = -1.
 // Queries whose search width was narrowed by the partition (width < r) and that found
-// fewer than K neighbors inside it are appended to a fallback list; a second pass of
-// this kernel re-searches them at the full radius, so every row is exact.
+// fewer than K neighbors inside it are flagged; the driver compacts them into a list that
+// the next pass (this kernel or k_search_q below) searches at a wider width, and the last
+// pass at the full radius, so every row is exact.
 #include "common.cuh"
 #include "kernels.h"
 
