@@ -9,7 +9,7 @@
 //   kCountingSortIndices + sortByKey(pos, particles) (grid.cu:312-329, sort.cpp:612):
 //     here a direct scatter into cell-sorted float4 {x, y, z, index} (no radix sort).
 //   ToCellIndex_MortonMetaGrid / MortonCode3 (grid.cu:13-31, helper_mortonCode.h:19-33):
-//     Morton keys of queries (queries are then radix-sorted, radix_sort.cu).
+//     Hilbert-curve keys of queries (queries are then radix-sorted, radix_sort.cu).
 #include "common.cuh"
 #include "kernels.h"
 
