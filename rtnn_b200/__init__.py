@@ -26,6 +26,8 @@ FLAG_SORTED_ROWS = 0x8
 FLAG_LOCAL_INDICES = 0x10
 FLAG_ANY_K = 0x20
 MAX_K = 128
+MODEL_FEATURES = 6   # RTNN_MODEL_FEATURES
+MODEL_NORM_PARAMS = 2 * MODEL_FEATURES + 2   # RTNN_MODEL_NORM_PARAMS
 
 _STATUS = {
     0: "RTNN_OK", 1: "RTNN_ERR_INVALID_ARGUMENT", 2: "RTNN_ERR_CUDA",
@@ -296,7 +298,7 @@ class Context:
         """(features [Q, 6], targets [Q]) as CUDA tensors from one plain search."""
         import torch
         nq = points.shape[0] if queries is None else queries.shape[0]
-        feats = torch.empty((nq, 6), dtype=torch.float32, device=points.device)
+        feats = torch.empty((nq, MODEL_FEATURES), dtype=torch.float32, device=points.device)
         tgt = torch.empty((nq,), dtype=torch.float32, device=points.device)
         self._check(load_library().rtnn_collect_training(
             self._h, _P(points.data_ptr()), points.shape[0],
@@ -325,7 +327,7 @@ class Context:
 
     def mlp_loss_grad(self, params, feats, target):
         import torch
-        n_train = self.model_size() - 14
+        n_train = self.model_size() - MODEL_NORM_PARAMS
         grad = torch.zeros(n_train, dtype=torch.float32, device=feats.device)
         loss = torch.zeros(1, dtype=torch.float32, device=feats.device)
         self._check(load_library().rtnn_mlp_loss_grad(

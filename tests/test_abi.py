@@ -50,6 +50,14 @@ def test_model_size_matches_layout():
     assert lib.rtnn_model_size() == 2 * F + 2 + H * F + H + H * H + H + H + 1
 
 
+def test_python_model_constants_match_header():
+    hdr = open(os.path.join(ROOT, "include", "rtnn_learn.h")).read()
+    feats = int(re.search(r"#define RTNN_MODEL_FEATURES (\d+)", hdr).group(1))
+    norm = int(re.search(r"#define RTNN_MODEL_NORM_PARAMS (\d+)", hdr).group(1))
+    assert (feats, norm) == (rtnn_b200.MODEL_FEATURES, rtnn_b200.MODEL_NORM_PARAMS)
+    assert norm == 2 * feats + 2
+
+
 def _have_gpu():
     try:
         import torch

@@ -151,3 +151,28 @@ def test_learned_widths_are_tighter_than_analytic(ctx):
     print(f"mean search volume analytic {vol_a:.3f} learned {vol_l:.3f}, fallback {fb_rate:.3%}")
     assert vol_l < vol_a
     assert fb_rate < 0.25
+
+
+def test_width_features_match_oracle_box_counts(ctx):
+    """The shell-count features of the width model (N_0..N_2 box counts around a query's
+    cell) equal the oracle's counts on the same grid (cell and origin from the search)."""
+    import torch
+    p = wl.uniform_cube(20000, 30.0, seed=12)
+    tp = torch.from_numpy(p).cuda()
+    st = rtnn_b200.Stats()
+    ctx.search(tp, None, "knn", 2.0, 16, partition=True, stats=st)
+    f, _ = ctx.collect_training(tp, None, "knn", 2.0, 16)
+    f = f.cpu().numpy()
+    assert f.shape == (p.shape[0], rtnn_b200.MODEL_FEATURES)
+    cell = np.float32(st.cell_size)
+    dims = np.array(list(st.grid_dims))
+    o = p.min(0).astype(np.float32)
+    inv = np.float32(1) / cell
+    ci = np.clip(np.floor((p - o) * inv), 0, dims - 1).astype(np.int64)
+    counts = np.zeros(dims[::-1], dtype=np.uint32)
+    np.add.at(counts, (ci[:, 2], ci[:, 1], ci[:, 0]), 1)
+    for i in range(0, p.shape[0], 37):
+        N = oracle.box_counts(counts, *ci[i], shells=3).astype(np.float64)
+        exp = np.log1p([N[0], N[1] - N[0], N[2] - N[1]])
+        assert np.allclose(f[i, [0, 1, 2]], exp, atol=1e-5), (i, f[i], N)
+        assert abs(f[i, 3] - (np.log(17.0) - np.log1p(N[2]))) <= 1e-5
