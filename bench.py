@@ -153,7 +153,7 @@ def train_model(ctx, cfg, scale, rank):
     perm = torch.randperm(f.shape[0], device=f.device, generator=torch.Generator(device=f.device).manual_seed(0))
     f = f[perm].contiguous()
     t = t[perm].contiguous()
-    losses = ctx.train_model(f, t, epochs=8, batch=16384, lr=3e-3, seed=rank)
+    losses = ctx.train_model(f, t, epochs=32, batch=16384, lr=3e-3, seed=rank)
     return {"samples": int(f.shape[0]), "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
 
 
