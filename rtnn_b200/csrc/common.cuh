@@ -116,20 +116,8 @@ __device__ __forceinline__ int clamp_cell(float c, int d) {
   return (int)c;
 }
 
-// 10-bit-per-axis Morton interleave (bit i of x -> bit 3i).
-__device__ __forceinline__ uint32_t spread3(uint32_t x) {
-  x &= 0x3ffu;
-  x = (x | (x << 16)) & 0x030000ffu;
-  x = (x | (x << 8)) & 0x0300f00fu;
-  x = (x | (x << 4)) & 0x030c30c3u;
-  x = (x | (x << 2)) & 0x09249249u;
-  return x;
-}
-__device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
-  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
-}
-
-// 21-bit-per-axis Morton interleave into 64 bits (same bit convention).
+// 21-bit-per-axis Morton interleave into 64 bits (bit i of x -> bit 3i, y -> 3i+1, z -> 3i+2,
+// the reference's convention, helper_mortonCode.h:30-33).
 __device__ __forceinline__ uint64_t spread3_64(uint64_t x) {
   x &= 0x1fffffull;
   x = (x | (x << 32)) & 0x001f00000000ffffull;
