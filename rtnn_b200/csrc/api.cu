@@ -623,8 +623,8 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
     const Shapes& sh = shs[g];
     RTNN_CU(cudaMemcpyAsync(c->ws.tables.p, sh.tab.data(), sh.tab.size() * 4, cudaMemcpyHostToDevice, s),
             "copy tables");
-    if (sh.N == 0) {
-      RTNN_CU(cudaMemsetAsync(d_out + qoff[cut[g]] * pr.k, 0xff, sh.Q * pr.k * 4, s), "fill output");
+    if (sh.N == 0 || sh.Q == 0) {   // nothing to search: empty rows (if any), no counts
+      if (sh.Q) RTNN_CU(cudaMemsetAsync(d_out + qoff[cut[g]] * pr.k, 0xff, sh.Q * pr.k * 4, s), "fill output");
       RTNN_CU(cudaMemsetAsync(d_sub + g, 0, sizeof(Counters), s), "clear counters");
       for (int i = 0; i < 5; ++i) RTNN_CU(cudaEventRecord(c->sub_ev[g][i], s), "event");
     } else {
@@ -672,11 +672,11 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
       if (partitioned(pr)) stats->n_fallback += h[g].fb_count[0];
       stats->n_tiles += sh.n_tiles;
       stats->n_cells += h[g].total_cells;
-      stats->n_launches += sh.N ? launches_of(sh, pr, false) : 0;
+      stats->n_launches += (sh.N && sh.Q) ? launches_of(sh, pr, false) : 0;
       stats->n_loaded += h[g].n_loaded;
       stats->n_tested += h[g].n_tested;
       float t[5] = {0, 0, 0, 0, 0};
-      if (sh.N) {
+      if (sh.N && sh.Q) {
         cudaEventElapsedTime(&t[0], c->sub_ev[g][0], c->sub_ev[g][1]);
         cudaEventElapsedTime(&t[1], c->sub_ev[g][1], c->sub_ev[g][2]);
         cudaEventElapsedTime(&t[2], c->sub_ev[g][2], c->sub_ev[g][4]);
