@@ -11,7 +11,8 @@
 //      nearby queries, see below);
 //   2. the candidate cells are the grid box covering bbox +- R; in raster order each
 //      (y, z) row of that box is one contiguous range of the cell-sorted points, so a
-//      row costs two offset loads (computed lane-parallel, 32 rows at a time);
+//      row costs two offset loads (computed lane-parallel, 32 rows at a time); rows, and
+//      the ends of rows, farther than R from the bbox are skipped (RowClip);
 //   3. 32 rows at a time are streamed as one flattened candidate sequence with 16-byte
 //      loads (rows in a stride-permuted order), the points farther than R from the tile
 //      box are dropped, and the survivors are compacted with __ballot_sync into a
@@ -102,6 +103,75 @@ constexpr int kCheck = 4;          // candidates tested between two buffer-full 
 constexpr uint32_t kQueryCap = 128;   // k_search_q hit buffer per warp (k <= 64)
 constexpr int kStage = 64;         // staged candidates per warp (float4)
 constexpr uint64_t kRowStride = 4294967311ull;   // prime > 2^32 > any row count of a box
+
+// Cell rows of a candidate box clipped to the points within R of the query box, in cell
+// units: c(v) = (v - origin) * inv_cell with the rounding that bins the points, so a point
+// of cell i has i <= c(p) < i + 1 along each axis. [X0, X1] x [Y0, Y1] x [Z0, Z1] is the
+// query box (one point for a single query) in those units. A point within R of a query
+// of the box lies in a row (cy, cz) whose cell square is within Rc = R * inv_cell of the
+// box's (y, z) rectangle, and inside that row in the cells floor(X0 - e) .. floor(X1 + e)
+// with e = sqrt(Rc^2 - gap_y^2 - gap_z^2). Every extent is widened by s, which exceeds the
+// FP32 rounding of the map (a few ulps of the largest coordinate) and of this arithmetic,
+// so a row or cell is only ever dropped when none of its points can be a hit.
+struct RowClip {
+  float X0, X1, Y0, Y1, Z0, Z1, Rs2, s;
+  __device__ __forceinline__ RowClip(const CloudGrid& g, float bx0, float bx1, float by0,
+                                     float by1, float bz0, float bz1, float R) {
+    X0 = __fmul_rn(__fsub_rn(bx0, g.ox), g.inv_cell);
+    X1 = __fmul_rn(__fsub_rn(bx1, g.ox), g.inv_cell);
+    Y0 = __fmul_rn(__fsub_rn(by0, g.oy), g.inv_cell);
+    Y1 = __fmul_rn(__fsub_rn(by1, g.oy), g.inv_cell);
+    Z0 = __fmul_rn(__fsub_rn(bz0, g.oz), g.inv_cell);
+    Z1 = __fmul_rn(__fsub_rn(bz1, g.oz), g.inv_cell);
+    const float Rc = __fmul_ru(R, g.inv_cell);
+    const float M = fmaxf(fmaxf(fmaxf(fabsf(X0), fabsf(X1)), fmaxf(fabsf(Y0), fabsf(Y1))),
+                          fmaxf(fabsf(Z0), fabsf(Z1)));
+    s = 0.01f + 1e-6f * (M + Rc);
+    const float Rs = __fadd_ru(Rc, s);
+    Rs2 = __fmul_ru(Rs, Rs);
+  }
+  // The cells [xl, xh] of row (cy, cz) within the box's x range [lx, hx]; false: none.
+  __device__ __forceinline__ bool row(int cy, int cz, int lx, int hx, int& xl, int& xh) const {
+    const float fy = (float)cy, fz = (float)cz;
+    const float gy = fmaxf(fmaxf(Y0 - (fy + 1.f + s), (fy - s) - Y1), 0.f);
+    const float gz = fmaxf(fmaxf(Z0 - (fz + 1.f + s), (fz - s) - Z1), 0.f);
+    const float rem = Rs2 - (gy * gy + gz * gz);
+    if (!(rem >= 0.f)) return false;
+    const float r2 = fmaxf(rem, 1e-20f);
+    const float e = r2 * rsqrtf(r2) + s;   // sqrt within a few ulps, far inside s
+    xl = max(__float2int_rd(X0 - e), lx);
+    xh = min(__float2int_rd(X1 + e), hx);
+    return xl <= xh;
+  }
+};
+
+// RowClip of a single query (a box of one point): three coordinates instead of six, so
+// the per-query walk keeps its registers.
+struct RowClipPoint {
+  float X, Y, Z, Rs2, s;
+  __device__ __forceinline__ RowClipPoint(const CloudGrid& g, float qx, float qy, float qz,
+                                          float R) {
+    X = __fmul_rn(__fsub_rn(qx, g.ox), g.inv_cell);
+    Y = __fmul_rn(__fsub_rn(qy, g.oy), g.inv_cell);
+    Z = __fmul_rn(__fsub_rn(qz, g.oz), g.inv_cell);
+    const float Rc = __fmul_ru(R, g.inv_cell);
+    s = 0.01f + 1e-6f * (fmaxf(fmaxf(fabsf(X), fabsf(Y)), fabsf(Z)) + Rc);
+    const float Rs = __fadd_ru(Rc, s);
+    Rs2 = __fmul_ru(Rs, Rs);
+  }
+  __device__ __forceinline__ bool row(int cy, int cz, int lx, int hx, int& xl, int& xh) const {
+    const float fy = (float)cy, fz = (float)cz;
+    const float gy = fmaxf(fmaxf(Y - (fy + 1.f + s), (fy - s) - Y), 0.f);
+    const float gz = fmaxf(fmaxf(Z - (fz + 1.f + s), (fz - s) - Z), 0.f);
+    const float rem = Rs2 - (gy * gy + gz * gz);
+    if (!(rem >= 0.f)) return false;
+    const float r2 = fmaxf(rem, 1e-20f);
+    const float e = r2 * rsqrtf(r2) + s;
+    xl = max(__float2int_rd(X - e), lx);
+    xh = min(__float2int_rd(X + e), hx);
+    return xl <= xh;
+  }
+};
 
 // Hit window on the bits of a non-negative FP32 distance d (bit order == value order):
 // radius: d < lim;  KNN: 0 < d < lim;  and, once the heap is full, d <= root distance
@@ -289,6 +359,7 @@ k_search(SearchArgs a) {
       const int lz = (int)fmaxf(fz0, 0.f), hz = (int)fminf(fz1, (float)(g.dz - 1));
       const int ny = hy - ly + 1, nz = hz - lz + 1;
       const int nrows = empty ? 0 : ny * nz;
+      const RowClip clip(g, bx0, bx1, by0, by1, bz0, bz1, R);
 
       const float lim_l = act ? lim : -1.f;
       LaneTop top{~0ull, 0u, 0u};
@@ -406,9 +477,12 @@ k_search(SearchArgs a) {
           // appended counts level and the merges short
           const int rq = (int)(((uint64_t)ri * kRowStride) % (uint64_t)nrows);
           const int cy = ly + rq % ny, cz = lz + rq / ny;
-          const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
-          rs = __ldg(a.cells + rowc + lx);
-          re = __ldg(a.cells + rowc + hx + 1);
+          int xl, xh;
+          if (clip.row(cy, cz, lx, hx, xl, xh)) {
+            const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+            rs = __ldg(a.cells + rowc + xl);
+            re = __ldg(a.cells + rowc + xh + 1);
+          }
         }
         // the (up to) 32 rows as one sequence of candidates: an inclusive scan of the row
         // lengths; candidate t belongs to the row whose scanned end is the first above t
@@ -536,7 +610,9 @@ k_search(SearchArgs a) {
 // The alternative walk for narrow widths: a warp takes a tile of 32 sorted queries like
 // k_search but searches them one after another, each over its own candidate box only
 // (a tile box holds many times more points than the box of one of its queries). The
-// box's cell rows are flattened 64 candidates at a time, two per lane (prefix sum of the
+// box's cell rows, clipped to the ball of radius R around the query (RowClipPoint: a
+// third fewer candidates than the cube), are flattened 64 candidates at a time, two per
+// lane (prefix sum of the
 // row lengths, shuffle search for a candidate's row), every lane tests its candidates
 // against the query, and the hits are compacted into a per-warp buffer in shared memory
 // with ballots. When the buffer could overflow, and at the end when it holds more than
@@ -692,6 +768,7 @@ k_search_q(SearchArgs a) {
       const int lz = (int)fmaxf(fz0, 0.f), hz = (int)fminf(fz1, (float)(g.dz - 1));
       const int ny = hy - ly + 1, nz = hz - lz + 1;
       const int nrows = empty ? 0 : ny * nz;
+      const RowClipPoint clip(g, qx, qy, qz, R);
 
       uint32_t wlo, wspan;   // hit window on the distance bits (see hit_window)
       hit_window(true, limj, INFINITY, KNN, wlo, wspan);
@@ -700,11 +777,12 @@ k_search_q(SearchArgs a) {
       for (int rb = 0; rb < nrows && !stop; rb += 32) {
         uint32_t rs = 0, re = 0;
         const int ri = rb + lane;
-        if (ri < nrows) {
+        int xl, xh;
+        if (ri < nrows && clip.row(ly + ri % ny, lz + ri / ny, lx, hx, xl, xh)) {
           const int cy = ly + ri % ny, cz = lz + ri / ny;
           const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
-          rs = __ldg(a.cells + rowc + lx);
-          re = __ldg(a.cells + rowc + hx + 1);
+          rs = __ldg(a.cells + rowc + xl);
+          re = __ldg(a.cells + rowc + xh + 1);
         }
         const uint32_t len = re - rs;
         uint32_t incl = len;

@@ -380,6 +380,31 @@ def test_query_warps_match_oracle(ctx, k, qw):
         ctx.set_tuning(**base)
 
 
+@pytest.mark.parametrize("cell_ratio", [1.0 / 3.0, 0.5, 1.0])
+def test_clipped_rows_keep_points_at_the_radius(ctx, cell_ratio):
+    """The walks skip cell rows (and the ends of rows) that lie entirely farther than the
+    search width from the query box. Lattice points far from the origin (4096 + i / 4,
+    where the cell map rounds most) sit on or next to cell boundaries, and r is a hair above
+    three lattice steps, so many neighbors lie exactly at the edge of the ball: every
+    kernel choice, with the partition off and on, must return the oracle's rows."""
+    base = ctx.tuning().as_dict()
+    g = np.stack(np.meshgrid(np.arange(24), np.arange(24), np.arange(24), indexing="ij"), -1)
+    p = (4096.0 + g.reshape(-1, 3) / 4.0).astype(np.float32)
+    q = np.concatenate([p[::7], p[::11] + np.float32(0.125)]).astype(np.float32)
+    r = float(np.nextafter(np.float32(0.75), np.float32(1)))
+    try:
+        for qw in (0, 1, 2):
+            ctx.set_tuning(**{**base, "cell_ratio": cell_ratio, "points_per_cell": 0.0,
+                              "query_warps": qw})
+            for mode, k in (("knn", 32), ("radius", 128)):
+                exp = oracle.grid_search(p, q, mode, r, k)
+                for part in (False, True):
+                    got = ctx.search(p, q, mode, r, k, partition=part, sorted_rows=True)
+                    assert_rows_equal(got, exp, True)
+    finally:
+        ctx.set_tuning(**base)
+
+
 def test_bounded_wait_reports_timeout_and_context_survives(ctx):
     """A device-side wait that can never be satisfied (a scan predecessor nobody
     publishes) gives up after its limit and reports RTNN_ERR_DEVICE_TIMEOUT; the context
