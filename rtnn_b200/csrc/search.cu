@@ -112,7 +112,12 @@ constexpr uint64_t kRowStride = 4294967311ull;   // prime > 2^32 > any row count
 // box's (y, z) rectangle, and inside that row in the cells floor(X0 - e) .. floor(X1 + e)
 // with e = sqrt(Rc^2 - gap_y^2 - gap_z^2). Every extent is widened by s, which exceeds the
 // FP32 rounding of the map (a few ulps of the largest coordinate) and of this arithmetic,
-// so a row or cell is only ever dropped when none of its points can be a hit.
+// so a row or cell is only ever dropped when none of its points can be a hit. Past 2^23
+// cells (coordinates without a fraction left, or a width far beyond any grid, where the
+// squares could overflow) the clip is off: coordinates 0, s = inf and Rs2 = 1 make every
+// gap 0 and e infinite, and the saturating float-to-int conversion then gives the whole
+// row [lx, hx] of the box.
+constexpr float kClipLimit = 8388608.f;
 struct RowClip {
   float X0, X1, Y0, Y1, Z0, Z1, Rs2, s;
   __device__ __forceinline__ RowClip(const CloudGrid& g, float bx0, float bx1, float by0,
@@ -129,6 +134,11 @@ struct RowClip {
     s = 0.01f + 1e-6f * (M + Rc);
     const float Rs = __fadd_ru(Rc, s);
     Rs2 = __fmul_ru(Rs, Rs);
+    if (!(M + Rc < kClipLimit)) {
+      X0 = X1 = Y0 = Y1 = Z0 = Z1 = 0.f;
+      s = INFINITY;
+      Rs2 = 1.f;
+    }
   }
   // The cells [xl, xh] of row (cy, cz) within the box's x range [lx, hx]; false: none.
   __device__ __forceinline__ bool row(int cy, int cz, int lx, int hx, int& xl, int& xh) const {
@@ -155,9 +165,15 @@ struct RowClipPoint {
     Y = __fmul_rn(__fsub_rn(qy, g.oy), g.inv_cell);
     Z = __fmul_rn(__fsub_rn(qz, g.oz), g.inv_cell);
     const float Rc = __fmul_ru(R, g.inv_cell);
-    s = 0.01f + 1e-6f * (fmaxf(fmaxf(fabsf(X), fabsf(Y)), fabsf(Z)) + Rc);
+    const float M = fmaxf(fmaxf(fabsf(X), fabsf(Y)), fabsf(Z));
+    s = 0.01f + 1e-6f * (M + Rc);
     const float Rs = __fadd_ru(Rc, s);
     Rs2 = __fmul_ru(Rs, Rs);
+    if (!(M + Rc < kClipLimit)) {   // off, as in RowClip
+      X = Y = Z = 0.f;
+      s = INFINITY;
+      Rs2 = 1.f;
+    }
   }
   __device__ __forceinline__ bool row(int cy, int cz, int lx, int hx, int& xl, int& xh) const {
     const float fy = (float)cy, fz = (float)cz;

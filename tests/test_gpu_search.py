@@ -405,6 +405,25 @@ def test_clipped_rows_keep_points_at_the_radius(ctx, cell_ratio):
         ctx.set_tuning(**base)
 
 
+def test_clip_off_for_widths_beyond_the_grid(ctx):
+    """A radius of 1e20 over a unit cloud with cells of a few hundredths (min_cell_ratio
+    1e-25 lets the cells stay small): the width is ~1e21 cells, where squares overflow
+    FP32, so the row clip must switch itself off and walk every row. r * r is infinite,
+    so every point qualifies and the rows are the K nearest."""
+    base = ctx.tuning().as_dict()
+    u = wl.uniform_cube(2000, 1.0, seed=3)
+    try:
+        for qw in (0, 1):
+            ctx.set_tuning(**{**base, "cell_ratio": 0.125, "min_cell_ratio": 1e-25,
+                              "points_per_cell": 0.125, "query_warps": qw})
+            for mode, k in (("radius", 128), ("knn", 32), ("knn", 64)):
+                exp = oracle.bruteforce(u, None, mode, 1e20, k)
+                got = ctx.search(u, None, mode, 1e20, k, sorted_rows=True)
+                assert_rows_equal(got, exp, True)
+    finally:
+        ctx.set_tuning(**base)
+
+
 def test_bounded_wait_reports_timeout_and_context_survives(ctx):
     """A device-side wait that can never be satisfied (a scan predecessor nobody
     publishes) gives up after its limit and reports RTNN_ERR_DEVICE_TIMEOUT; the context
