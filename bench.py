@@ -38,6 +38,10 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # profiles/k_search_knn_multicloud_scale0.1.md (1,102 MB for 5.25 M queries), scaled by
 # queries to a full launch; only known for the default workload.
 TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 210.0}
+# Warp instructions per query of the first search pass (smsp__inst_executed.sum over the
+# queries in the same capture: 5.141e9 for 5.25 M queries). The search is bound by
+# instruction issue, not DRAM, so the bench also reports the issue rate this implies.
+INST_PER_QUERY = {"knn_multicloud_4096": 979.0}
 
 
 def parse():
@@ -437,11 +441,12 @@ def run_rtnn(args, rank, world):
 
     # dominant kernel (search, both passes) timed with the library's events on `stream`
     nog = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=False, **common)
-    ms_search, ms_build, ms_part = [], [], []
+    ms_search, ms_build, ms_part, ms_fb = [], [], [], []
     for _ in range(max(3, args.steps)):
         s2 = rtnn_b200.Stats()
         nog.execute(tp, tq, out, stats=s2)
         ms_search.append(s2.ms_search)
+        ms_fb.append(s2.ms_fallback)
         ms_build.append(s2.ms_build)
         ms_part.append(s2.ms_partition)
     nog.close()
@@ -457,6 +462,19 @@ def run_rtnn(args, rank, world):
                 "traffic_scope": "main search pass, ncu at scale 0.1 scaled by queries",
                 "kernel": "k_search (all passes)", "peak_source": pk_src,
                 "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": round(ms_s, 4)}
+    ms_main = ms_s - statistics.mean(ms_fb)
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
+    if args.workload in INST_PER_QUERY and mhz and ms_main > 0:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        ach = INST_PER_QUERY[args.workload] * Q / (ms_main * 1e-3)
+        peak = sms * 4 * float(mhz) * 1e6   # one warp instruction per scheduler per cycle
+        roofline["issue"] = {
+            "warp_inst_per_query": INST_PER_QUERY[args.workload],
+            "achieved": round(ach / 1e12, 4), "peak": round(peak / 1e12, 4),
+            "unit": "T warp-inst/s", "frac": round(ach / peak, 3), "ms_first_pass": round(ms_main, 4),
+            "scope": "first search pass (k_search): instructions per query from ncu at scale "
+                     "0.1, time from the library's CUDA events, peak = SMs x 4 schedulers x "
+                     "median sampled SM clock"}
 
     e2e = None
     if not args.no_e2e:
