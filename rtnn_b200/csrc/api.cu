@@ -73,7 +73,7 @@ struct Shapes {
   std::vector<uint32_t> tab;  // batched: point_off | query_off | chunk_base | qchunk_base | tile_base
   uint32_t n_chunks = 0, n_qchunks = 0, n_tiles = 0;
   uint64_t max_cloud_q = 0;
-  uint32_t morton_bits = 1, key_bits = 8;
+  uint32_t order_bits = 1, key_bits = 8;
   bool key64 = false;
   float cell_budget = 8.f;
   uint64_t cell_capacity = 0;
@@ -170,7 +170,7 @@ void finish_shapes(Shapes& sh, const rtnn_tuning& tu) {
   const uint32_t cb = ceil_log2(sh.n_clouds);
   if (cb + 3 * mb + 4 > 64) mb = (60 - cb) / 3;   // room for 4 density-bucket bits
   if (mb > 1 && cb + 3 * mb + 4 > 32 && cb + 3 * (mb - 1) + 4 <= 32) --mb;   // stay 32-bit
-  sh.morton_bits = mb;
+  sh.order_bits = mb;
   sh.key_bits = std::max(8u, cb + 3 * mb);
   sh.key64 = sh.key_bits > 32;
   // cells: each cloud gets max(64, budget * points); indices stay 32-bit
@@ -326,7 +326,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
 
   RTNN_CU(launch_bbox(d_pts, sh.N, ap, t, sh.n_chunks, (uint32_t*)ws.bbox.p, s), "bbox");
   RTNN_CU(launch_grid_plan(t, (const uint32_t*)ws.bbox.p, pr.radius, tu.cell_ratio,
-                           tu.min_cell_ratio, tu.points_per_cell, sh.cell_budget, sh.morton_bits, sh.cell_capacity, grids, ctr, s),
+                           tu.min_cell_ratio, tu.points_per_cell, sh.cell_budget, sh.order_bits, sh.cell_capacity, grids, ctr, s),
           "grid plan");
   RTNN_CU(launch_zero_cells(cells, ctr, c->n_sms, s), "zero cells");
   RTNN_CU(launch_count(d_pts, sh.N, ap, t, sh.n_chunks, grids, cells, (uint32_t*)ws.rank.p, ctr, s),
@@ -364,7 +364,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     RTNN_CU(launch_widths(w, c->n_sms, s), "widths");
   }
   const bool key64 = key64_of(sh, pr);
-  RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.morton_bits,
+  RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.order_bits,
                             part ? (const float*)ws.qwidth_in.p : nullptr, pr.radius,
                             level_bits_of(pr), tu.buckets_per_halving, key64, ws.keys0.p, s),
           "query keys");

@@ -120,7 +120,7 @@ k_bbox(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cloud
 __global__ void __launch_bounds__(1024)
 k_grid_plan(CloudTables t, const uint32_t* __restrict__ bbox, float radius, float cell_ratio,
             float min_cell_ratio, float points_per_cell, float cell_budget,
-            uint32_t morton_bits, uint64_t cell_capacity, CloudGrid* __restrict__ grids,
+            uint32_t order_bits, uint64_t cell_capacity, CloudGrid* __restrict__ grids,
             Counters* ctr) {
   __shared__ uint32_t s_sum[32];
   __shared__ uint64_t s_carry;
@@ -175,10 +175,10 @@ k_grid_plan(CloudTables t, const uint32_t* __restrict__ bbox, float radius, floa
       g.cell = cell; g.inv_cell = 1.0f / cell;
       g.dx = d[0]; g.dy = d[1]; g.dz = d[2];
       g.n_cells = (uint32_t)((uint64_t)d[0] * d[1] * d[2]);
-      // query order: Hilbert index on 2^morton_bits steps across the cloud's longest side
+      // query order: Hilbert index on 2^order_bits steps across the cloud's longest side
       // (finer than the cells, so dense cells still yield compact 32-query tiles)
       const float ext = fmaxf(fmaxf(mx[0] - mn[0], mx[1] - mn[1]), fmaxf(mx[2] - mn[2], 1e-30f));
-      g.morton_scale = (float)((1u << morton_bits) - 1u) / ext;
+      g.order_scale = (float)((1u << order_bits) - 1u) / ext;
       ncell = g.n_cells;
     }
     // block-wide exclusive scan of ncell (values < 2^32, carry kept in 64 bits)
@@ -286,22 +286,22 @@ __device__ __forceinline__ uint32_t width_level(float w, float radius, uint32_t 
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
 k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
-             CloudTables t, const CloudGrid* __restrict__ grids, uint32_t morton_bits,
+             CloudTables t, const CloudGrid* __restrict__ grids, uint32_t order_bits,
              const float* __restrict__ qwidth, float radius, uint32_t level_bits,
              float per_halving, KeyT* __restrict__ keys) {
   __shared__ float s_xyz[kChunk * 3];
   const ChunkRange r = chunk_range(t.qchunk_base, t.query_off, t.n_clouds, blockIdx.x);
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
   const CloudGrid g = grids[r.cloud];
-  const int top = (int)((1u << morton_bits) - 1u);
+  const int top = (int)((1u << order_bits) - 1u);
   for (uint32_t i = threadIdx.x; i < r.end - r.begin; i += blockDim.x) {
-    const int fx = clamp_cell(cell_coord_f(s_xyz[3 * i], g.ox, g.morton_scale), top + 1);
-    const int fy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.morton_scale), top + 1);
-    const int fz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.morton_scale), top + 1);
-    const uint64_t m = hilbert3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz, morton_bits);
+    const int fx = clamp_cell(cell_coord_f(s_xyz[3 * i], g.ox, g.order_scale), top + 1);
+    const int fy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.order_scale), top + 1);
+    const int fz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.order_scale), top + 1);
+    const uint64_t m = hilbert3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz, order_bits);
     const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits, per_halving) : 0u;
-    keys[r.begin + i] = ((KeyT)r.cloud << (3 * morton_bits + level_bits)) |
-                        ((KeyT)lvl << (3 * morton_bits)) | (KeyT)m;
+    keys[r.begin + i] = ((KeyT)r.cloud << (3 * order_bits + level_bits)) |
+                        ((KeyT)lvl << (3 * order_bits)) | (KeyT)m;
   }
 }
 
@@ -347,10 +347,10 @@ cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const
 
 cudaError_t launch_grid_plan(const CloudTables& t, const uint32_t* bbox, float radius,
                              float cell_ratio, float min_cell_ratio, float points_per_cell,
-                             float cell_budget, uint32_t morton_bits, uint64_t cell_capacity,
+                             float cell_budget, uint32_t order_bits, uint64_t cell_capacity,
                              CloudGrid* grids, Counters* ctr, cudaStream_t s) {
   k_grid_plan<<<1, 1024, 0, s>>>(t, bbox, radius, cell_ratio, min_cell_ratio, points_per_cell,
-                                 cell_budget, morton_bits, cell_capacity, grids, ctr);
+                                 cell_budget, order_bits, cell_capacity, grids, ctr);
   return cudaGetLastError();
 }
 
@@ -379,17 +379,17 @@ cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
 
 cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
                               const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
-                              uint32_t morton_bits, const float* qwidth, float radius,
+                              uint32_t order_bits, const float* qwidth, float radius,
                               uint32_t level_bits, float per_halving, bool key64, void* keys,
                               cudaStream_t s) {
   if (n_qchunks == 0) return cudaSuccess;
   if (key64)
     k_query_keys<uint64_t><<<n_qchunks, 256, 0, s>>>(xyz, 3 * n_queries, aligned, t, grids,
-                                                     morton_bits, qwidth, radius, level_bits,
+                                                     order_bits, qwidth, radius, level_bits,
                                                      per_halving, (uint64_t*)keys);
   else
     k_query_keys<uint32_t><<<n_qchunks, 256, 0, s>>>(xyz, 3 * n_queries, aligned, t, grids,
-                                                     morton_bits, qwidth, radius, level_bits,
+                                                     order_bits, qwidth, radius, level_bits,
                                                      per_halving, (uint32_t*)keys);
   return cudaGetLastError();
 }

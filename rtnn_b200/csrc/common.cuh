@@ -6,7 +6,8 @@
 //                      grid cell (raster order inside each cloud, clouds in order).
 //   cells              uint32 per cell + 1: per-cell counts, scanned in place into
 //                      cell start offsets (cells[total] == number of points).
-//   sq                 float4 {x, y, z, original query index bits} in Morton order.
+//   sq                 float4 {x, y, z, original query index bits} in (cloud, density
+//                      bucket, Hilbert index) order.
 //   out (caller)       int32 [Q][K], -1 in unused slots.
 #pragma once
 #include <cstdint>
@@ -40,7 +41,7 @@ struct __align__(16) CloudGrid {
   float inv_cell;        // 1 / cell
   int dx, dy, dz;        // cells per axis
   uint32_t cell_base;    // first cell of this cloud in the global cell array
-  float morton_scale;    // query order: Morton code of floor((x - origin) * morton_scale)
+  float order_scale;    // query order: Hilbert index of floor((x - origin) * order_scale)
   uint32_t n_cells;      // dx * dy * dz
   uint32_t pad;
 };

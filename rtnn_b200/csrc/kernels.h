@@ -16,7 +16,7 @@ struct SearchArgs {
   const CloudGrid* grids;
   const uint32_t* cells;       // cell start offsets (scanned counts)
   const float4* spts;          // cell-sorted points {x, y, z, index}
-  const float4* sq;            // Morton-sorted queries {x, y, z, query index}
+  const float4* sq;            // sorted queries (cloud, bucket, Hilbert) {x, y, z, query index}
   const float* qwidth;         // per sorted query search width; nullptr: full radius
   // fallback passes read the list the previous pass wrote (sorted position, cloud,
   // width to search at) ...
@@ -69,7 +69,7 @@ cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const
                         uint32_t n_chunks, uint32_t* bbox, cudaStream_t s);
 cudaError_t launch_grid_plan(const CloudTables& t, const uint32_t* bbox, float radius,
                              float cell_ratio, float min_cell_ratio, float points_per_cell,
-                             float cell_budget, uint32_t morton_bits, uint64_t cell_capacity,
+                             float cell_budget, uint32_t order_bits, uint64_t cell_capacity,
                              CloudGrid* grids, Counters* ctr, cudaStream_t s);
 cudaError_t launch_zero_cells(uint32_t* cells, const Counters* ctr, int n_sms, cudaStream_t s);
 cudaError_t launch_count(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
@@ -81,7 +81,7 @@ cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
                            Counters* ctr, cudaStream_t s);
 cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
                               const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
-                              uint32_t morton_bits, const float* qwidth, float radius,
+                              uint32_t order_bits, const float* qwidth, float radius,
                               uint32_t level_bits, float per_halving, bool key64, void* keys,
                               cudaStream_t s);
 cudaError_t launch_gather_queries(const float* xyz, const uint32_t* order, uint32_t n,

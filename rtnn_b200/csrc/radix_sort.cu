@@ -2,9 +2,9 @@
 //
 // Replaces the CUB radix sorts behind thrust::sort_by_key in the reference
 // (thrust_helper.cu:13-43; call sites sort.cpp:415,487-488,612). Used to put queries
-// in Morton order. Each pass: (1) per-tile digit histograms, column-major
-// [digit][tile]; (2) one exclusive scan of that table (scan.cu), giving every
-// (digit, tile) its global output offset; (3) a stable scatter: each warp ranks its
+// in (cloud, density bucket, Hilbert index) order. Each pass: (1) per-tile digit
+// histograms, column-major [digit][tile]; (2) one exclusive scan of that table (scan.cu),
+// giving every (digit, tile) its global output offset; (3) a stable scatter: each warp ranks its
 // sub-tile with __match_any_sync, warps are combined through a shared-memory prefix per
 // digit, the tile is placed in digit order in shared memory, and written out from there
 // so that consecutive threads write consecutive output positions of a digit's run (keys
