@@ -64,6 +64,13 @@ typedef enum rtnn_mode {
 #define RTNN_FLAG_ANY_K           0x20u /* any K of the qualifying points (the first found),
                                            not the K nearest: the reference's radius-search
                                            semantics (geometry.cu:72-83), cheaper */
+#define RTNN_FLAG_KEEP_ORDER      0x40u /* plans only (time stepping, points that move a little
+                                           between executes): the first execute sorts the
+                                           queries and keeps that order, later executes reuse it
+                                           and skip the query keys and sort (the reference
+                                           sorts the queries on every run, sort.cpp:393-498,
+                                           751-797); rows stay exact, only tile coherence can
+                                           age. See rtnn_plan_resort. */
 
 /* Per-call statistics (all optional to read). Times are device times measured with
  * CUDA events on the context stream (graph replays report ms_total only). */
@@ -146,6 +153,9 @@ rtnn_status rtnn_plan_create(rtnn_ctx* ctx, rtnn_plan** plan,
 rtnn_status rtnn_plan_execute(rtnn_plan* plan, const float* d_points, const float* d_queries,
                               int32_t* d_out, rtnn_stats* stats);
 rtnn_status rtnn_plan_destroy(rtnn_plan* plan);
+/* RTNN_FLAG_KEEP_ORDER plans: the next execute sorts the queries again (for example every
+ * few time steps, or after the points moved far) and keeps the new order. */
+rtnn_status rtnn_plan_resort(rtnn_plan* plan);
 
 /* Search-tuning knobs chosen by the autotuner (rtnn_b200/autotune.py caches them). */
 typedef struct rtnn_tuning {

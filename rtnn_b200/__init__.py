@@ -15,7 +15,8 @@ import numpy as np
 
 __all__ = ["RtnnError", "Stats", "Tuning", "Context", "Plan", "search", "search_batched",
            "RADIUS", "KNN", "FLAG_DEVICE_POINTERS", "FLAG_PARTITION", "FLAG_LEARNED",
-           "FLAG_SORTED_ROWS", "FLAG_LOCAL_INDICES", "MAX_K", "library_path", "load_library"]
+           "FLAG_SORTED_ROWS", "FLAG_LOCAL_INDICES", "FLAG_ANY_K", "FLAG_KEEP_ORDER", "MAX_K",
+           "library_path", "load_library"]
 
 RADIUS = 0
 KNN = 1
@@ -25,6 +26,7 @@ FLAG_LEARNED = 0x4
 FLAG_SORTED_ROWS = 0x8
 FLAG_LOCAL_INDICES = 0x10
 FLAG_ANY_K = 0x20
+FLAG_KEEP_ORDER = 0x40
 MAX_K = 128
 MODEL_FEATURES = 6   # RTNN_MODEL_FEATURES
 MODEL_NORM_PARAMS = 2 * MODEL_FEATURES + 2   # RTNN_MODEL_NORM_PARAMS
@@ -103,6 +105,7 @@ _SIGS = {
     "rtnn_plan_create": (_I, [_P, ctypes.POINTER(_P), _P, _U32, _P, _I, _F, _U32, _U32, _I]),
     "rtnn_plan_execute": (_I, [_P, _P, _P, _P, ctypes.POINTER(Stats)]),
     "rtnn_plan_destroy": (_I, [_P]),
+    "rtnn_plan_resort": (_I, [_P]),
     "rtnn_model_size": (_U32, []),
     "rtnn_model_set": (_I, [_P, _P, _U32]),
     "rtnn_model_get": (_I, [_P, _P, _U32]),
@@ -277,9 +280,12 @@ class Context:
 
     def plan(self, point_offsets, query_offsets=None, mode="knn", radius=0.2, k=32,
              partition=False, learned=False, sorted_rows=False, local_indices=False,
-             use_graph=True, any_k=False):
+             use_graph=True, any_k=False, keep_order=False):
+        """keep_order (RTNN_FLAG_KEEP_ORDER): the first execute sorts the queries and later
+        executes reuse that order, skipping the query keys and sort (time stepping);
+        Plan.resort() makes the next execute sort again."""
         return Plan(self, point_offsets, query_offsets, mode, radius, k, partition, learned,
-                    sorted_rows, local_indices, use_graph, any_k)
+                    sorted_rows, local_indices, use_graph, any_k, keep_order)
 
     # -- learned widths -------------------------------------------------------------------
     def model_size(self):
@@ -352,14 +358,14 @@ class Plan:
     """Fixed-shape batched search replayed from a CUDA graph (rtnn_plan_*)."""
 
     def __init__(self, ctx, point_offsets, query_offsets, mode, radius, k, partition, learned,
-                 sorted_rows, local_indices, use_graph, any_k=False):
+                 sorted_rows, local_indices, use_graph, any_k=False, keep_order=False):
         self.ctx = ctx
         lib = load_library()
         po = np.ascontiguousarray(np.asarray(point_offsets, dtype=np.uint64))
         qo = None if query_offsets is None else np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64))
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
                  (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0) |
-                 (FLAG_ANY_K if any_k else 0))
+                 (FLAG_ANY_K if any_k else 0) | (FLAG_KEEP_ORDER if keep_order else 0))
         self.k = k
         self.n_queries = int((qo if qo is not None else po)[-1])
         h = _P()
@@ -379,6 +385,10 @@ class Plan:
             self._h, _P(points.data_ptr()), _P(queries.data_ptr()) if queries is not None else None,
             _P(out.data_ptr()), ctypes.byref(st)))
         return out
+
+    def resort(self):
+        """The next execute sorts the queries again (keep_order plans)."""
+        self.ctx._check(load_library().rtnn_plan_resort(self._h))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -57,6 +57,7 @@ struct Workspace {
   DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth,
       qwidth_in, fbflag, fbnextw, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters, in_pts, in_qs, out, feats,
       cellsz, kth;
+  bool order_in1 = false;   // the last query sort left its permutation in vals1 (else vals0)
   void release_all() {
     for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
                       &vals1, &sq, &qwidth, &qwidth_in, &fbflag, &fbnextw, &fbpos[0], &fbpos[1], &fbcloud[0], &fbcloud[1],
@@ -122,11 +123,14 @@ struct rtnn_plan {
   Params pr{};
   Workspace ws;
   bool use_graph = false;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  const float* g_pts = nullptr;
-  const float* g_qs = nullptr;
-  int32_t* g_out = nullptr;
+  bool keep_order = false;   // RTNN_FLAG_KEEP_ORDER
+  bool have_order = false;   // a sort ran and its order is kept (until rtnn_plan_resort)
+  // one graph per mode: [0] sorts the queries, [1] reuses the kept order
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  const float* g_pts[2] = {nullptr, nullptr};
+  const float* g_qs[2] = {nullptr, nullptr};
+  int32_t* g_out[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -148,7 +152,7 @@ rtnn_status cuda_fail(rtnn_ctx* c, cudaError_t e, const char* where) {
   } while (0)
 
 rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32_t k,
-                       uint32_t flags) {
+                       uint32_t flags, bool plan = false) {
   if (!(std::isfinite(radius) && radius >= 1e-30f))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "radius must be a finite number > 0");
   if (!rtnn_k_supported(k))
@@ -157,7 +161,10 @@ rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 points and queries");
   const uint32_t known = RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED |
                          RTNN_FLAG_SORTED_ROWS | RTNN_FLAG_LOCAL_INDICES | RTNN_FLAG_ANY_K;
-  if (flags & ~known) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "unknown flag bits");
+  if ((flags & RTNN_FLAG_KEEP_ORDER) && !plan)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "RTNN_FLAG_KEEP_ORDER applies to plans only");
+  if (flags & ~(known | RTNN_FLAG_KEEP_ORDER))
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "unknown flag bits");
   if ((flags & RTNN_FLAG_LEARNED) && !c->has_model)
     return fail(c, RTNN_ERR_NO_MODEL, "RTNN_FLAG_LEARNED needs a width model (rtnn_model_set or rtnn_model_train)");
   return RTNN_OK;
@@ -299,9 +306,10 @@ CloudTables tables_of(const Workspace& ws, uint32_t n_clouds) {
 
 // Issues the whole pipeline on stream s. ev: 4 events (or nullptr) bracketing
 // build | partition | search.
-uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats) {
+uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats, bool reuse_order = false) {
   const uint32_t passes = sh.Q ? (key_bits_of(sh, pr) + 7) / 8 : 0;
-  uint32_t n = (sh.single ? 1 : 0) + 7 + 3 * passes + 1;   // tables, build, sort, gather
+  // tables, build (6), query keys + sort (skipped when a kept order is reused), gather
+  uint32_t n = (sh.single ? 1 : 0) + 6 + (reuse_order ? 0 : 1 + 3 * passes) + 1;
   if (partitioned(pr) || feats) n += 1;                      // widths
   // search passes; each flagging pass adds a flag scan and a compaction
   n += partitioned(pr) ? 3 * fallback_passes_of(pr) + 4 : 1;
@@ -311,7 +319,7 @@ uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats) {
 rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr,
                   const float* d_pts, const float* d_qs, int32_t* d_out, cudaStream_t s,
                   cudaEvent_t* ev, float* feats_out = nullptr, float* cellsz_out = nullptr,
-                  uint32_t index_base = 0) {
+                  uint32_t index_base = 0, bool reuse_order = false) {
   Counters* ctr = (Counters*)ws.counters.p;
   const bool knn = pr.mode == RTNN_MODE_KNN;
   const rtnn_tuning& tu = c->tuning;
@@ -363,18 +371,24 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     w.cellsz = cellsz_out;
     RTNN_CU(launch_widths(w, c->n_sms, s), "widths");
   }
-  const bool key64 = key64_of(sh, pr);
-  RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.order_bits,
-                            part ? (const float*)ws.qwidth_in.p : nullptr, pr.radius,
-                            level_bits_of(pr), tu.buckets_per_halving, key64, ws.keys0.p, s),
-          "query keys");
-  bool in1 = false;
-  RTNN_CU(radix_sort_pairs(key64, ws.keys0.p, (uint32_t*)ws.vals0.p, ws.keys1.p,
-                           (uint32_t*)ws.vals1.p, (uint32_t)sh.Q, key_bits_of(sh, pr), true,
-                           (uint32_t*)ws.hist.p, (uint64_t*)ws.scan_state.p, &ctr->scan_tiles[1],
-                           ctr, &in1, s),
-          "radix sort");
-  const uint32_t* order = (const uint32_t*)(in1 ? ws.vals1.p : ws.vals0.p);
+  // reuse_order (a RTNN_FLAG_KEEP_ORDER plan after its first execute): the permutation of
+  // the last sort is still in vals0/vals1 and only the gather below runs; any order that
+  // keeps each cloud's queries together gives the same rows
+  if (!reuse_order) {
+    const bool key64 = key64_of(sh, pr);
+    RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.order_bits,
+                              part ? (const float*)ws.qwidth_in.p : nullptr, pr.radius,
+                              level_bits_of(pr), tu.buckets_per_halving, key64, ws.keys0.p, s),
+            "query keys");
+    bool in1 = false;
+    RTNN_CU(radix_sort_pairs(key64, ws.keys0.p, (uint32_t*)ws.vals0.p, ws.keys1.p,
+                             (uint32_t*)ws.vals1.p, (uint32_t)sh.Q, key_bits_of(sh, pr), true,
+                             (uint32_t*)ws.hist.p, (uint64_t*)ws.scan_state.p, &ctr->scan_tiles[1],
+                             ctr, &in1, s),
+            "radix sort");
+    ws.order_in1 = in1;
+  }
+  const uint32_t* order = (const uint32_t*)(ws.order_in1 ? ws.vals1.p : ws.vals0.p);
   RTNN_CU(launch_gather_queries(d_qs, order, (uint32_t)sh.Q, (float4*)ws.sq.p,
                                 part ? (const float*)ws.qwidth_in.p : nullptr,
                                 part ? (float*)ws.qwidth.p : nullptr, c->n_sms, s),
@@ -464,7 +478,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
 }
 
 rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& sh,
-                      const Params& pr, rtnn_stats* stats, bool timed) {
+                      const Params& pr, rtnn_stats* stats, bool timed, bool reuse_order = false) {
   RTNN_CU(cudaMemcpyAsync(c->h_ctr, ws.counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s),
           "read counters");
   RTNN_CU(cudaMemcpyAsync(c->h_grid, ws.grids.p, sizeof(CloudGrid), cudaMemcpyDeviceToHost, s),
@@ -491,7 +505,7 @@ rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& 
     stats->grid_dims[0] = (uint32_t)c->h_grid->dx;
     stats->grid_dims[1] = (uint32_t)c->h_grid->dy;
     stats->grid_dims[2] = (uint32_t)c->h_grid->dz;
-    stats->n_launches = launches_of(sh, pr, false);
+    stats->n_launches = launches_of(sh, pr, false, reuse_order);
     stats->n_loaded = h.n_loaded;
     stats->n_tested = h.n_tested;
     if (timed) {
@@ -844,12 +858,14 @@ rtnn_status rtnn_plan_create(rtnn_ctx* c, rtnn_plan** plan, const uint64_t* poin
   rtnn_plan* p = new rtnn_plan();
   p->ctx = c;
   rtnn_status st = batched_shapes(c, point_offsets, n_clouds, query_offsets, c->tuning, p->sh);
-  if (st == RTNN_OK) st = check_args(c, p->sh.N, p->sh.Q, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS);
+  if (st == RTNN_OK)
+    st = check_args(c, p->sh.N, p->sh.Q, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS, true);
   if (st == RTNN_OK && (p->sh.N == 0 || p->sh.Q == 0))
     st = fail(c, RTNN_ERR_INVALID_ARGUMENT, "a plan needs at least one point and one query");
   if (st != RTNN_OK) { delete p; return st; }
   p->pr = Params{mode, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS, c->tuning.fallback_passes};
   p->use_graph = use_graph != 0;
+  p->keep_order = (flags & RTNN_FLAG_KEEP_ORDER) != 0;
   cudaSetDevice(c->device);
   st = reserve(c, p->ws, p->sh, p->pr);
   if (st == RTNN_OK) {
@@ -876,40 +892,55 @@ rtnn_status rtnn_plan_execute(rtnn_plan* p, const float* d_points, const float* 
   cudaSetDevice(c->device);
   cudaStream_t s = stream_of(c);
   const float* d_qs = d_queries ? d_queries : d_points;
+  const bool reuse = p->keep_order && p->have_order;
   if (!p->use_graph) {
-    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, c->ev);
+    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, c->ev, nullptr,
+                           nullptr, 0, reuse);
     if (st != RTNN_OK) return st;
-    return read_back(c, p->ws, s, p->sh, p->pr, stats, true);
+    st = read_back(c, p->ws, s, p->sh, p->pr, stats, true, reuse);
+    if (st == RTNN_OK && p->keep_order) p->have_order = true;
+    return st;
   }
-  if (!p->exec || p->g_pts != d_points || p->g_qs != d_qs || p->g_out != d_out) {
-    if (p->exec) { cudaGraphExecDestroy(p->exec); p->exec = nullptr; }
-    if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  const int m = reuse ? 1 : 0;
+  if (!p->exec[m] || p->g_pts[m] != d_points || p->g_qs[m] != d_qs || p->g_out[m] != d_out) {
+    if (p->exec[m]) { cudaGraphExecDestroy(p->exec[m]); p->exec[m] = nullptr; }
+    if (p->graph[m]) { cudaGraphDestroy(p->graph[m]); p->graph[m] = nullptr; }
     RTNN_CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, nullptr);
+    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, nullptr, nullptr,
+                           nullptr, 0, reuse);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (st != RTNN_OK) { if (g) cudaGraphDestroy(g); return st; }
     if (e != cudaSuccess) return cuda_fail(c, e, "end capture");
-    p->graph = g;
-    RTNN_CU(cudaGraphInstantiate(&p->exec, g, 0), "instantiate graph");
-    p->g_pts = d_points;
-    p->g_qs = d_qs;
-    p->g_out = d_out;
+    p->graph[m] = g;
+    RTNN_CU(cudaGraphInstantiate(&p->exec[m], g, 0), "instantiate graph");
+    p->g_pts[m] = d_points;
+    p->g_qs[m] = d_qs;
+    p->g_out[m] = d_out;
   }
   RTNN_CU(cudaEventRecord(c->ev[0], s), "event");
-  RTNN_CU(cudaGraphLaunch(p->exec, s), "graph launch");
+  RTNN_CU(cudaGraphLaunch(p->exec[m], s), "graph launch");
   RTNN_CU(cudaEventRecord(c->ev[4], s), "event");
-  rtnn_status st = read_back(c, p->ws, s, p->sh, p->pr, stats, false);
+  rtnn_status st = read_back(c, p->ws, s, p->sh, p->pr, stats, false, reuse);
   if (st == RTNN_OK && stats) cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[4]);
+  if (st == RTNN_OK && p->keep_order) p->have_order = true;
   return st;
+}
+
+rtnn_status rtnn_plan_resort(rtnn_plan* p) {
+  if (!p) return RTNN_ERR_INVALID_ARGUMENT;
+  p->have_order = false;
+  return RTNN_OK;
 }
 
 rtnn_status rtnn_plan_destroy(rtnn_plan* p) {
   if (!p) return RTNN_OK;
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(stream_of(p->ctx));
-  if (p->exec) cudaGraphExecDestroy(p->exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
+  for (int m = 0; m < 2; ++m) {
+    if (p->exec[m]) cudaGraphExecDestroy(p->exec[m]);
+    if (p->graph[m]) cudaGraphDestroy(p->graph[m]);
+  }
   p->ws.release_all();
   delete p;
   return RTNN_OK;

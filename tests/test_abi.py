@@ -58,6 +58,15 @@ def test_python_model_constants_match_header():
     assert norm == 2 * feats + 2
 
 
+def test_python_flags_match_header():
+    hdr = open(os.path.join(ROOT, "include", "rtnn.h")).read()
+    flags = dict(re.findall(r"#define RTNN_FLAG_(\w+)\s+(0x[0-9a-fA-F]+)u", hdr))
+    assert {"DEVICE_POINTERS", "ANY_K", "KEEP_ORDER"} <= set(flags)
+    for name, value in flags.items():
+        assert getattr(rtnn_b200, "FLAG_" + name) == int(value, 16), name
+    assert len(set(flags.values())) == len(flags)
+
+
 def _have_gpu():
     try:
         import torch

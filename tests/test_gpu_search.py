@@ -290,6 +290,53 @@ def test_plan_graph_replay(ctx):
         plan.close()
 
 
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_plan_keep_order_time_steps(ctx, use_graph):
+    """KEEP_ORDER plans sort the queries on the first execute only and reuse that order
+    (no query keys, no sort) while the points move: rows stay exact through small steps,
+    through a shuffle of the positions inside every cloud (the kept order then means
+    nothing), and after resort(), which sorts once more."""
+    import ctypes
+    import torch
+    p, off = wl.multicloud(n_clouds=24, lo=64, hi=3000, seed=9)
+    rng = np.random.default_rng(4)
+    for flags in ({}, {"partition": True}):
+        cur = p.copy()
+        tp = torch.from_numpy(cur).cuda()
+        plan = ctx.plan(off, mode="knn", radius=0.2, k=16, use_graph=use_graph,
+                        sorted_rows=True, keep_order=True, **flags)
+        launches = []
+        for step in range(4):
+            st = rtnn_b200.Stats()
+            out = plan.execute(tp, stats=st)
+            launches.append(st.n_launches)
+            exp = oracle.grid_search_batched(cur, off, mode="knn", r=0.2, k=16)
+            assert np.array_equal(out.cpu().numpy(), exp), f"step {step}"
+            if step == 1:
+                for c in range(len(off) - 1):
+                    a, b = int(off[c]), int(off[c + 1])
+                    cur[a:b] = cur[a:b][rng.permutation(b - a)]
+            else:
+                cur = (cur + rng.normal(0.0, 0.005, cur.shape)).astype(np.float32)
+            tp.copy_(torch.from_numpy(cur))
+        assert launches[1] < launches[0] and launches[1] == launches[2] == launches[3]
+        plan.resort()
+        st = rtnn_b200.Stats()
+        out = plan.execute(tp, stats=st)
+        assert st.n_launches == launches[0]
+        exp = oracle.grid_search_batched(cur, off, mode="knn", r=0.2, k=16)
+        assert np.array_equal(out.cpu().numpy(), exp)
+        plan.close()
+    # the flag belongs to plans: a one-shot search rejects it
+    lib = rtnn_b200.load_library()
+    q = wl.uniform_cube(10, 1.0, seed=0)
+    res = np.empty((10, 4), np.int32)
+    st = lib.rtnn_search(ctx._h, q.ctypes.data_as(ctypes.c_void_p), 10, None, 10,
+                         rtnn_b200.KNN, 1.0, 4, rtnn_b200.FLAG_KEEP_ORDER,
+                         res.ctypes.data_as(ctypes.c_void_p), None)
+    assert st != 0
+
+
 def test_fp64_disagreement_is_only_boundary_pairs(ctx):
     rng = np.random.default_rng(9)
     p = (rng.integers(0, 40, (3000, 3)) * 0.25).astype(np.float32)
