@@ -154,7 +154,8 @@ def train_model(ctx, cfg, scale, rank):
         tgts.append(t)
     f = torch.cat(feats)
     t = torch.cat(tgts)
-    perm = torch.randperm(f.shape[0], device=f.device, generator=torch.Generator(device=f.device).manual_seed(0))
+    gen = torch.Generator(device=f.device).manual_seed(0)
+    perm = torch.randperm(f.shape[0], device=f.device, generator=gen)
     f = f[perm].contiguous()
     t = t[perm].contiguous()
     losses = ctx.train_model(f, t, epochs=32, batch=16384, lr=3e-3, seed=rank)
@@ -266,11 +267,12 @@ def cpu_reference_sample(cfg, seconds, threads, seed=0):
         done_q += nq
         if elapsed >= seconds:
             break
+    how = ("check.cpp sanityCheckKNN via oracle/_ref/refcheck" if use_ref
+           else "oracle restatement of check.cpp:34-48")
     return {"value": done_q / max(elapsed, 1e-9), "unit": "queries/s", "cores": threads,
             "kind": "reference" if use_ref else "port",
             "sample": f"{done_q} queries of the workload, brute force over their own cloud "
-                      f"({'check.cpp sanityCheckKNN via oracle/_ref/refcheck' if use_ref else 'oracle restatement of check.cpp:34-48'}), "
-                      f"{elapsed:.1f} s on {threads} host threads"}
+                      f"({how}), {elapsed:.1f} s on {threads} host threads"}
 
 
 def reduce_max(x, dist=None, device="cpu"):
@@ -487,7 +489,8 @@ def run_rtnn(args, rank, world):
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            ctx.search_batched(hp_np, cfg["offsets"], hq_np, cfg["qoffsets"], learned=True, out=ho_np, **common)
+            ctx.search_batched(hp_np, cfg["offsets"], hq_np, cfg["qoffsets"], learned=True,
+                               out=ho_np, **common)
         dt = max_over_ranks((time.perf_counter() - t0) / args.steps)
         h2d = 12 * N + (0 if hq is None else 12 * Q)
         e2e = {"value": world * Q / dt, "unit": "queries/s", "h2d_bytes_per_step": h2d,

@@ -250,7 +250,8 @@ class Context:
         """Many independent clouds in one launch; offsets have n_clouds + 1 entries."""
         lib = load_library()
         po = np.ascontiguousarray(np.asarray(point_offsets, dtype=np.uint64))
-        qo = None if query_offsets is None else np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64))
+        qo = (None if query_offsets is None
+              else np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64)))
         n_clouds = po.shape[0] - 1
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
                  (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0) |
@@ -362,7 +363,8 @@ class Plan:
         self.ctx = ctx
         lib = load_library()
         po = np.ascontiguousarray(np.asarray(point_offsets, dtype=np.uint64))
-        qo = None if query_offsets is None else np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64))
+        qo = (None if query_offsets is None
+              else np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64)))
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
                  (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0) |
                  (FLAG_ANY_K if any_k else 0) | (FLAG_KEEP_ORDER if keep_order else 0))

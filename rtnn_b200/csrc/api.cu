@@ -55,13 +55,13 @@ void release(DevBuf& b) {
 
 struct Workspace {
   DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth,
-      qwidth_in, fbflag, fbnextw, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters, in_pts, in_qs, out, feats,
-      cellsz, kth;
+      qwidth_in, fbflag, fbnextw, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters,
+      in_pts, in_qs, out, feats, cellsz, kth;
   bool order_in1 = false;   // the last query sort left its permutation in vals1 (else vals0)
   void release_all() {
     for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
-                      &vals1, &sq, &qwidth, &qwidth_in, &fbflag, &fbnextw, &fbpos[0], &fbpos[1], &fbcloud[0], &fbcloud[1],
-                      &fbwidth[0], &fbwidth[1], &hist, &scan_state, &counters,
+                      &vals1, &sq, &qwidth, &qwidth_in, &fbflag, &fbnextw, &fbpos[0], &fbpos[1],
+                      &fbcloud[0], &fbcloud[1], &fbwidth[0], &fbwidth[1], &hist, &scan_state, &counters,
                       &in_pts, &in_qs, &out, &feats, &cellsz, &kth})
       release(*b);
   }
@@ -166,7 +166,8 @@ rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32
   if (flags & ~(known | RTNN_FLAG_KEEP_ORDER))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "unknown flag bits");
   if ((flags & RTNN_FLAG_LEARNED) && !c->has_model)
-    return fail(c, RTNN_ERR_NO_MODEL, "RTNN_FLAG_LEARNED needs a width model (rtnn_model_set or rtnn_model_train)");
+    return fail(c, RTNN_ERR_NO_MODEL,
+                "RTNN_FLAG_LEARNED needs a width model (rtnn_model_set or rtnn_model_train)");
   return RTNN_OK;
 }
 
@@ -334,7 +335,8 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
 
   RTNN_CU(launch_bbox(d_pts, sh.N, ap, t, sh.n_chunks, (uint32_t*)ws.bbox.p, s), "bbox");
   RTNN_CU(launch_grid_plan(t, (const uint32_t*)ws.bbox.p, pr.radius, tu.cell_ratio,
-                           tu.min_cell_ratio, tu.points_per_cell, sh.cell_budget, sh.order_bits, sh.cell_capacity, grids, ctr, s),
+                           tu.min_cell_ratio, tu.points_per_cell, sh.cell_budget, sh.order_bits,
+                           sh.cell_capacity, grids, ctr, s),
           "grid plan");
   RTNN_CU(launch_zero_cells(cells, ctr, c->n_sms, s), "zero cells");
   RTNN_CU(launch_count(d_pts, sh.N, ap, t, sh.n_chunks, grids, cells, (uint32_t*)ws.rank.p, ctr, s),
@@ -486,11 +488,14 @@ rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& 
   RTNN_CU(cudaStreamSynchronize(s), "synchronize");
   const Counters& h = *c->h_ctr;
   if (h.error == kErrScanTimeout)
-    return fail(c, RTNN_ERR_DEVICE_TIMEOUT, "scan look-back gave up waiting on tile " + std::to_string(h.error_info));
+    return fail(c, RTNN_ERR_DEVICE_TIMEOUT,
+                "scan look-back gave up waiting on tile " + std::to_string(h.error_info));
   if (h.error == kErrCellCapacity)
-    return fail(c, RTNN_ERR_INTERNAL, "grid plan exceeded its cell capacity (cloud " + std::to_string(h.error_info) + ")");
+    return fail(c, RTNN_ERR_INTERNAL,
+                "grid plan exceeded its cell capacity (cloud " + std::to_string(h.error_info) + ")");
   if (h.error == kErrIndexRange)
-    return fail(c, RTNN_ERR_INTERNAL, "device index check failed (element " + std::to_string(h.error_info) + ")");
+    return fail(c, RTNN_ERR_INTERNAL,
+                "device index check failed (element " + std::to_string(h.error_info) + ")");
   if (h.error != 0) return fail(c, RTNN_ERR_INTERNAL, "device error " + std::to_string(h.error));
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
@@ -638,7 +643,8 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
     RTNN_CU(cudaMemcpyAsync(c->ws.tables.p, sh.tab.data(), sh.tab.size() * 4, cudaMemcpyHostToDevice, s),
             "copy tables");
     if (sh.N == 0 || sh.Q == 0) {   // nothing to search: empty rows (if any), no counts
-      if (sh.Q) RTNN_CU(cudaMemsetAsync(d_out + qoff[cut[g]] * pr.k, 0xff, sh.Q * pr.k * 4, s), "fill output");
+      if (sh.Q)
+        RTNN_CU(cudaMemsetAsync(d_out + qoff[cut[g]] * pr.k, 0xff, sh.Q * pr.k * 4, s), "fill output");
       RTNN_CU(cudaMemsetAsync(d_sub + g, 0, sizeof(Counters), s), "clear counters");
       for (int i = 0; i < 5; ++i) RTNN_CU(cudaEventRecord(c->sub_ev[g][i], s), "event");
     } else {
@@ -661,14 +667,17 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
   RTNN_CU(cudaStreamSynchronize(c->copy), "synchronize");
   std::vector<Counters> h(G);
   RTNN_CU(cudaMemcpyAsync(h.data(), d_sub, G * sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
-  RTNN_CU(cudaMemcpyAsync(c->h_grid, c->ws.grids.p, sizeof(CloudGrid), cudaMemcpyDeviceToHost, s), "read grid");
+  RTNN_CU(cudaMemcpyAsync(c->h_grid, c->ws.grids.p, sizeof(CloudGrid), cudaMemcpyDeviceToHost, s),
+          "read grid");
   RTNN_CU(cudaStreamSynchronize(s), "synchronize");
   for (uint32_t g = 0; g < G; ++g) {
     const Counters& hc = h[g];
     if (hc.error == kErrScanTimeout)
-      return fail(c, RTNN_ERR_DEVICE_TIMEOUT, "scan look-back gave up waiting on tile " + std::to_string(hc.error_info));
+      return fail(c, RTNN_ERR_DEVICE_TIMEOUT,
+                  "scan look-back gave up waiting on tile " + std::to_string(hc.error_info));
     if (hc.error == kErrCellCapacity)
-      return fail(c, RTNN_ERR_INTERNAL, "grid plan exceeded its cell capacity (cloud " + std::to_string(cut[g] + hc.error_info) + ")");
+      return fail(c, RTNN_ERR_INTERNAL, "grid plan exceeded its cell capacity (cloud " +
+                                            std::to_string(cut[g] + hc.error_info) + ")");
     if (hc.error != 0) return fail(c, RTNN_ERR_INTERNAL, "device error " + std::to_string(hc.error));
   }
   if (stats) {
@@ -869,7 +878,8 @@ rtnn_status rtnn_plan_create(rtnn_ctx* c, rtnn_plan** plan, const uint64_t* poin
   cudaSetDevice(c->device);
   st = reserve(c, p->ws, p->sh, p->pr);
   if (st == RTNN_OK) {
-    cudaError_t e = cudaMemcpy(p->ws.tables.p, p->sh.tab.data(), p->sh.tab.size() * 4, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(p->ws.tables.p, p->sh.tab.data(), p->sh.tab.size() * 4,
+                               cudaMemcpyHostToDevice);
     if (e != cudaSuccess) st = cuda_fail(c, e, "copy tables");
   }
   if (st != RTNN_OK) {

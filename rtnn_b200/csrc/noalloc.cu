@@ -169,7 +169,8 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
   if (e == cudaSuccess)
     e = radix_sort_pairs(false, keys0, vals0, keys1, vals1, (uint32_t)Q, key_bits, true, hist,
                          scan_state, &ctr->scan_tiles[1], ctr, &in1, s);
-  if (e == cudaSuccess) e = launch_gather_queries(d_qs, in1 ? vals1 : vals0, (uint32_t)Q, sq, nullptr, nullptr, n_sms, s);
+  if (e == cudaSuccess)
+    e = launch_gather_queries(d_qs, in1 ? vals1 : vals0, (uint32_t)Q, sq, nullptr, nullptr, n_sms, s);
   if (e == cudaSuccess) {
     SearchArgs a{};
     a.t = t;

@@ -113,7 +113,8 @@ __device__ __forceinline__ void box_counts3(const CloudGrid& g, const uint32_t* 
     for (int dy = -2; dy <= 2; ++dy) {
       const int y = cy + dy;
       if (y < 0 || y >= g.dy) continue;
-      const uint32_t* row = cells + g.cell_base + ((uint32_t)z * (uint32_t)g.dy + (uint32_t)y) * (uint32_t)g.dx;
+      const uint32_t* row =
+          cells + g.cell_base + ((uint32_t)z * (uint32_t)g.dy + (uint32_t)y) * (uint32_t)g.dx;
       n2 += __ldg(row + x1 + 1) - __ldg(row + x0);
       if (dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
         n1 += __ldg(row + i1 + 1) - __ldg(row + i0);

@@ -151,14 +151,22 @@ cudaError_t radix_sort_pairs(bool key64, void* keys0, uint32_t* vals0, void* key
     const uint32_t* vin = (p == 0 && identity_values) ? nullptr : (in1 ? vals1 : vals0);
     uint32_t* vout = in1 ? vals0 : vals1;
     const uint32_t shift = 8 * p;
-    if (key64) k_radix_hist<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint64_t*)kin, n, shift, hist, n_tiles);
-    else k_radix_hist<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint32_t*)kin, n, shift, hist, n_tiles);
+    if (key64)
+      k_radix_hist<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint64_t*)kin, n, shift, hist,
+                                                                n_tiles);
+    else
+      k_radix_hist<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint32_t*)kin, n, shift, hist,
+                                                                n_tiles);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const uint64_t hn = 256ull * n_tiles;
     e = launch_scan_excl(hist, hn, nullptr, 0, hn, scan_state, scan_counters + p, ctr, s);
     if (e != cudaSuccess) return e;
-    if (key64) k_radix_scatter<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint64_t*)kin, vin, (uint64_t*)kout, vout, n, shift, hist, n_tiles);
-    else k_radix_scatter<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint32_t*)kin, vin, (uint32_t*)kout, vout, n, shift, hist, n_tiles);
+    if (key64)
+      k_radix_scatter<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>(
+          (const uint64_t*)kin, vin, (uint64_t*)kout, vout, n, shift, hist, n_tiles);
+    else
+      k_radix_scatter<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>(
+          (const uint32_t*)kin, vin, (uint32_t*)kout, vout, n, shift, hist, n_tiles);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     in1 = !in1;
   }

@@ -457,7 +457,8 @@ k_search(SearchArgs a) {
         while (true) {
           while (ptr >= end && ri < nrl) {   // next non-empty row of this lane's box
             const int cy = l1 + ri % nyl, cz = l2 + ri / nyl;
-            const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+            const uint32_t rowc =
+                g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
             ptr = __ldg(a.cells + rowc + l0);
             end = __ldg(a.cells + rowc + h0 + 1);
             ++ri;
@@ -495,7 +496,8 @@ k_search(SearchArgs a) {
           const int cy = ly + rq % ny, cz = lz + rq / ny;
           int xl, xh;
           if (clip.row(cy, cz, lx, hx, xl, xh)) {
-            const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+            const uint32_t rowc =
+                g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
             rs = __ldg(a.cells + rowc + xl);
             re = __ldg(a.cells + rowc + xh + 1);
           }
@@ -933,17 +935,20 @@ void fit_search_shape(uint32_t k, uint32_t pending_req, int wpb_req, uint32_t* p
 
 cudaError_t search_prepare(int device) {
   (void)device;
-  cudaError_t e = cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSearchSmemLimit);
+  cudaError_t e = cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSearchSmemLimit);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSearchSmemLimit);
+    e = cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSearchSmemLimit);
   return e;
 }
 
 int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block) {
   int nb = 0;
   const size_t smem = search_smem_bytes(k, pending, warps_per_block);
-  cudaError_t e = knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<true>, warps_per_block * 32, smem)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<false>, warps_per_block * 32, smem);
+  const int threads = warps_per_block * 32;
+  cudaError_t e = knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<true>, threads, smem)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<false>, threads, smem);
   if (e != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }
@@ -957,8 +962,10 @@ uint32_t search_q_cap(uint32_t k) { return k + 64 <= kQueryCap ? kQueryCap : 0u;
 int search_q_blocks_per_sm(bool knn, uint32_t k, int warps_per_block) {
   int nb = 0;
   const size_t smem = search_q_smem_bytes(search_q_cap(k), warps_per_block);
-  cudaError_t e = knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<true>, warps_per_block * 32, smem)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<false>, warps_per_block * 32, smem);
+  const int threads = warps_per_block * 32;
+  cudaError_t e =
+      knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<true>, threads, smem)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<false>, threads, smem);
   if (e != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }

@@ -32,7 +32,8 @@ def assert_rows_equal(got, exp, sorted_rows):
         bad = np.nonzero((got != exp).any(1))[0]
     else:
         bad = np.nonzero((as_sets(got) != as_sets(exp)).any(1))[0]
-    assert bad.size == 0, f"{bad.size} rows differ, first {bad[:5].tolist()}: got {got[bad[0]].tolist()} exp {exp[bad[0]].tolist()}"
+    assert bad.size == 0, (f"{bad.size} rows differ, first {bad[:5].tolist()}: "
+                           f"got {got[bad[0]].tolist()} exp {exp[bad[0]].tolist()}")
     # every row: the valid entries come first, then only -1
     valid = got >= 0
     assert (valid[:, :-1] | ~valid[:, 1:]).all()
