@@ -160,3 +160,27 @@ def test_batched_oracle_is_per_cloud():
         assert np.array_equal(rows[a:b], exp)
     local = oracle.grid_search_batched(p, off, mode="knn", r=0.3, k=6, local=True)
     assert local.max() < max(sizes)
+
+
+def test_grid_oracle_matches_bruteforce_on_edge_inputs():
+    """The grid oracle is the expected result of several GPU tests; on their edge inputs it
+    must equal the brute force: lattice points at a 4096 offset with neighbors exactly at
+    the radius (r a hair above three steps), coincident points, non-finite and far
+    queries (empty rows), a radius whose square is infinite in FP32, K = 1 and 128."""
+    g = np.stack(np.meshgrid(np.arange(12), np.arange(12), np.arange(12), indexing="ij"), -1)
+    lat = (4096.0 + g.reshape(-1, 3) / 4.0).astype(np.float32)
+    lq = np.concatenate([lat[::5], lat[::7] + np.float32(0.125)]).astype(np.float32)
+    r = float(np.nextafter(np.float32(0.75), np.float32(1)))
+    rng = np.random.default_rng(11)
+    dup = np.repeat(rng.uniform(0, 2, (40, 3)).astype(np.float32), 3, axis=0)
+    bad_q = np.array([[np.nan, 1, 1], [np.inf, 0, 0], [1e30, 0, 0], [1, 1, 1]], np.float32)
+    unit = rng.uniform(0, 1, (500, 3)).astype(np.float32)
+    cases = [(lat, lq, r), (dup, None, 0.3), (dup, bad_q, 0.5), (unit, None, 1e20)]
+    for p, q, rad in cases:
+        for mode in ("radius", "knn"):
+            for k in (1, 32, 128):
+                a = oracle.bruteforce(p, q, mode, rad, k)
+                b = oracle.grid_search(p, q, mode, rad, k)
+                assert np.array_equal(a, b), (len(p), mode, rad, k)
+    rows = oracle.bruteforce(dup, bad_q, "knn", 0.5, 8)
+    assert (rows[:3] == -1).all() and (rows[3] >= 0).any()
