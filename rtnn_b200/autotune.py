@@ -1,5 +1,10 @@
 """Autotuner for the search pipeline.
 
+Replaces the reference's fixed rules for the same choices: the cell/radius ratio derived
+from free GPU memory (calcCRRatio, util.cpp:551-676, used at util.cpp:680-688) and the
+partition cost model that groups queries into batches (autoBatchingRange /
+autoBatchingKNN, sort.cpp:221-320); here the choices are timed on the caller's data.
+
 Picks the tuning knobs of a context (include/rtnn.h, rtnn_tuning) for one workload by
 timing candidate settings on the GPU with the library's own event timers, one knob at a
 time (coordinate descent) after timing a few whole cell-size presets: the cell edge

@@ -3,7 +3,9 @@
 Compiles every .cu of rtnn_b200/csrc for sm_100a with nvcc and links them into
 rtnn_b200/lib/librtnn_b200.so (static cudart, C ABI of include/rtnn.h). The CLI
 rtnn_b200/bin/optixNSearch links against that library. Incremental: a target is rebuilt
-only when one of its sources or headers is newer.
+only when one of its sources or headers is newer. Stands in for the reference's CMake build
+of optixNSearch (src/optixNSearch/CMakeLists.txt); its compile-time KNN K (-DKNN, lines
+58-61) becomes the CLI's -DRTNN_KNN default, while the library takes K at run time.
 """
 import os
 import subprocess
