@@ -1,7 +1,7 @@
 """CPU oracle for the neighbor-search path -- TEST INFRASTRUCTURE ONLY.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and
-only as the checker or the timed CPU reference; the library (rtnn_b200) never imports it.
+only to check results or as the timed CPU reference; the library (rtnn_b200) never imports it.
 
 - liboracle.so (oracle.c): FP32 restatement of the reference's distance and predicates,
   brute force and grid-accelerated, plus an FP64 brute force and the FP32/FP64 boundary

@@ -2,7 +2,7 @@
  * oracle.c -- CPU restatement of the reference's neighbor-search semantics.
  *
  * TEST INFRASTRUCTURE ONLY: the parity tests, __graft_entry__.smoke() and the CPU
- * baseline of bench.py call this library as the checker. The product (librtnn_b200.so)
+ * baseline of bench.py call this library to check results. The product (librtnn_b200.so)
  * never links or calls it.
  *
  * Semantics restated (paths relative to the reference project):

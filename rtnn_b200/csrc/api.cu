@@ -1,4 +1,4 @@
-// api.cu -- C ABI (include/rtnn.h) and the host-side pipeline driver.
+// api.cu -- C ABI (include/rtnn.h) and the host side of the pipeline.
 //
 // The pipeline replaces the timed region of optixNSearch (src/optixNSearch/main.cpp:91-148):
 //   uploadData/computeMinMax (optix.cpp:117-168)      -> k_bbox, k_grid_plan

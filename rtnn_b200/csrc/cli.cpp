@@ -96,7 +96,8 @@ Options parse(int argc, char** argv) {
     else if (a == "--threads") o.threads = (unsigned)std::atoi(next().c_str());
     else if (ignored.count(a)) {
       const std::string v = next();
-      std::fprintf(stderr, "warning: %s %s has no effect in this build\n", a.c_str(), v.c_str());
+      std::fprintf(stderr, "warning: %s %s has no effect (accepted for compatibility)\n",
+                   a.c_str(), v.c_str());
     } else {
       std::fprintf(stderr, "Unknown option '%s'\n", a.c_str());
       usage(argv[0]);

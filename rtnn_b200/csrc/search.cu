@@ -23,9 +23,9 @@
 //      appended branch-free and merged into a max-heap of the K kept when a column fills;
 //   5. rows are written warp-cooperatively (coalesced), unused slots = -1.
 // Queries whose search width was narrowed by the partition (width < r) and that found
-// fewer than K neighbors inside it are flagged; the driver compacts them into a list that
-// the next pass (this kernel or k_search_q below) searches at a wider width, and the last
-// pass at the full radius, so every row is exact.
+// fewer than K neighbors inside it are flagged; the host pipeline compacts them into a
+// list that the next pass (this kernel or k_search_q below) searches at a wider width,
+// and the last pass at the full radius, so every row is exact.
 #include "common.cuh"
 #include "kernels.h"
 
