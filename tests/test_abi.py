@@ -96,3 +96,27 @@ def test_mode_names():
     assert rtnn_b200._mode("knn") == rtnn_b200.KNN
     with pytest.raises(ValueError):
         rtnn_b200._mode("nearest")
+
+
+def test_headers_are_c99_and_link_from_c(tmp_path):
+    """The public headers compile as strict C99 and a C program links against the library
+    (what a cgo or plain-C caller does); without a GPU, rtnn_create reports an error
+    status instead of crashing."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not found")
+    src = tmp_path / "caller.c"
+    src.write_text('#include "rtnn.h"\n#include "rtnn_learn.h"\n'
+                   "int main(void) {\n"
+                   "  rtnn_ctx* c = 0; rtnn_stats s; rtnn_tuning t; (void)s; (void)t;\n"
+                   "  rtnn_status st = rtnn_create(&c, 0);\n"
+                   "  if (st == RTNN_OK) { rtnn_destroy(c); return 0; }\n"
+                   "  return 1;\n}\n")
+    lib_dir = os.path.dirname(rtnn_b200.library_path())
+    exe = tmp_path / "caller"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                    "-I" + os.path.join(ROOT, "include"), str(src), "-L" + lib_dir,
+                    "-lrtnn_b200", "-Wl,-rpath," + lib_dir, "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, timeout=120)
+    assert r.returncode in (0, 1)
