@@ -42,6 +42,32 @@ TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 210.0}
 # queries in the same capture: 5.141e9 for 5.25 M queries). The search is bound by
 # instruction issue, not DRAM, so the bench also reports the issue rate this implies.
 INST_PER_QUERY = {"knn_multicloud_4096": 979.0}
+# Per-kernel ncu figures of one learned step plus one width-model training step of the
+# default workload at scale 0.1 (409 clouds, 5,250,132 points = queries), from the capture
+# summarised in profiles/kernels_knn_multicloud_scale0.1.md (gpu__time_duration.sum,
+# dram__bytes_read.sum + dram__bytes_write.sum; times are cold-cache and serialised):
+# kernel -> (launches, total us, DRAM bytes, algorithmic bytes per unit, unit).
+KERNEL_PROFILE = {"knn_multicloud_4096": {"units": 5250132, "kernels": {}}}
+
+
+def kernel_rooflines(workload):
+    """Per-kernel DRAM throughput from the committed ncu capture, against the measured HBM
+    peak; traffic scaled by units to one launch of the full workload."""
+    prof = KERNEL_PROFILE[workload]
+    pk, src = peaks()
+    full_units = {"knn_multicloud_4096": 54763252}.get(workload, prof["units"])
+    out = []
+    for name, (n, us, dram, alg_per_unit, unit) in prof["kernels"].items():
+        gbs = dram / (us * 1e-6) / 1e9 if us else 0.0
+        d = {"kernel": name, "launches": n, "ncu_us": us, "dram_gbs": round(gbs, 1),
+             "frac": round(gbs / pk["hbm_gbs"], 4), "peak_source": src,
+             "traffic_full_size": round(dram * full_units / prof["units"])}
+        if alg_per_unit:
+            alg = alg_per_unit * prof["units"]
+            d["algorithmic_bytes_per_" + unit] = alg_per_unit
+            d["algorithmic_frac"] = round(alg / (us * 1e-6) / 1e9 / pk["hbm_gbs"], 4)
+        out.append(d)
+    return out
 
 
 def parse():
@@ -56,15 +82,24 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink point counts (tests)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="time only --workload (by default the four other configurations "
+                         "follow, with fewer steps, under other_workloads)")
     ap.add_argument("--profile", action="store_true",
-                    help="train the width model, then run one learned step (no graph) between "
-                         "cudaProfilerStart/Stop, for ncu --profile-from-start off; no JSON line")
+                    help="train the width model, then run one learned step (no graph) and one "
+                         "training step of the width model (loss/gradient, Adam, inference) "
+                         "between cudaProfilerStart/Stop, for ncu --profile-from-start off; no "
+                         "JSON line")
+    ap.add_argument("--profile-path", default="learned", choices=["learned", "partition", "plain"],
+                    help="--profile: the step profiled (learned widths, the analytic partition "
+                         "or the plain grid)")
     return ap.parse_args()
 
 
 def run_profile(args):
-    """One learned step of the workload bracketed by cudaProfilerStart/Stop."""
+    """One step of the workload bracketed by cudaProfilerStart/Stop, followed (learned
+    path) by one training step of the width model: k_mlp_loss_grad, k_mlp_adam and
+    k_mlp_forward on the training samples, so that one capture lists every kernel."""
     import torch
     import rtnn_b200
     cfg = make_workload(args.workload, args.scale, 0)
@@ -75,20 +110,37 @@ def run_profile(args):
     ctx.set_tuning(points_per_cell=0.125, cell_ratio=0.125, min_cell_ratio=0.01, width_margin=1.1,
                    fallback_passes=2, gap_ratio=2.0, pending_slots=16, query_warps=2,
                    buckets_per_halving=1.0)
-    train_model(ctx, cfg, args.scale, 0)
+    learned = args.profile_path == "learned"
+    if learned:
+        train_model(ctx, cfg, args.scale, 0)
+        p0, q0 = training_clouds(cfg["name"], args.scale, 0)[0]
+        tp0 = torch.from_numpy(np.ascontiguousarray(p0)).cuda()
+        tq0 = None if q0 is None else torch.from_numpy(np.ascontiguousarray(q0)).cuda()
+        feats, tgt = ctx.collect_training(tp0, tq0, cfg["mode"], cfg["radius"], cfg["k"])
+        params = torch.from_numpy(ctx.get_model()).cuda()
+        n_train = params.numel() - rtnn_b200.MODEL_NORM_PARAMS
+        adam_m = torch.zeros(n_train, device="cuda")
+        adam_v = torch.zeros(n_train, device="cuda")
     tp = torch.from_numpy(cfg["points"]).cuda()
     tq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).cuda()
     out = torch.empty((cfg["n_queries"], cfg["k"]), dtype=torch.int32, device="cuda")
     plan = ctx.plan(cfg["offsets"], cfg["qoffsets"], mode=cfg["mode"], radius=cfg["radius"],
-                    k=cfg["k"], learned=True, use_graph=False)
+                    k=cfg["k"], learned=learned, partition=args.profile_path == "partition",
+                    use_graph=False)
     plan.execute(tp, tq, out)
     torch.cuda.synchronize()
     st = rtnn_b200.Stats()
     torch.cuda.profiler.start()
     plan.execute(tp, tq, out, stats=st)
+    if learned:
+        grad, _ = ctx.mlp_loss_grad(params, feats, tgt)
+        ctx.mlp_adam_step(params, grad, adam_m, adam_v, 1e-3, 1, 1.0 / feats.shape[0])
+        ctx.mlp_forward(params, feats)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
     print("profiled step:", json.dumps(st.as_dict()), flush=True)
+    if learned:
+        print(f"profiled training step: {feats.shape[0]} samples", flush=True)
     plan.close()
     ctx.close()
 
@@ -122,44 +174,12 @@ def make_workload(name, scale, rank):
 def training_clouds(name, scale, rank):
     """Clouds of other seeds (never the measured one) for the width model."""
     from rtnn_b200 import workloads as wl
-    s = 1000 * rank + 100
-    out = []
-    if name == "knn_multicloud_4096":
-        p, off = wl.multicloud(n_clouds=96, seed=s + 7)
-        for c in range(len(off) - 1):
-            out.append((p[int(off[c]):int(off[c + 1])], None))
-    elif name == "knn_surface_1e7":
-        for i in range(20):
-            out.append((wl.surfaces(seed=s + i, scale=0.05 * max(scale, 0.02)), None))
-    elif name == "knn_gmm_1e6":
-        for i in range(4):
-            out.append(wl.gmm(seed=s + i, scale=0.25 * scale))
-    elif name == "radius_uniform_1e5":
-        for i in range(4):
-            out.append((wl.uniform_cube(seed=s + i, scale=scale), None))
-    else:
-        for i in range(2):
-            out.append((wl.sph_lattice(seed=s + i, scale=0.02 * scale), None))
-    return out
+    return wl.training_clouds(name, scale, rank)
 
 
 def train_model(ctx, cfg, scale, rank):
-    import torch
-    feats, tgts = [], []
-    for p, q in training_clouds(cfg["name"], scale, rank):
-        tp = torch.from_numpy(np.ascontiguousarray(p)).cuda()
-        tq = None if q is None else torch.from_numpy(np.ascontiguousarray(q)).cuda()
-        f, t = ctx.collect_training(tp, tq, cfg["mode"], cfg["radius"], cfg["k"])
-        feats.append(f)
-        tgts.append(t)
-    f = torch.cat(feats)
-    t = torch.cat(tgts)
-    gen = torch.Generator(device=f.device).manual_seed(0)
-    perm = torch.randperm(f.shape[0], device=f.device, generator=gen)
-    f = f[perm].contiguous()
-    t = t[perm].contiguous()
-    losses = ctx.train_model(f, t, epochs=32, batch=16384, lr=3e-3, seed=rank)
-    return {"samples": int(f.shape[0]), "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+    from rtnn_b200 import workloads as wl
+    return wl.train_width_model(ctx, cfg["name"], scale, rank)
 
 
 # ---------------------------------------------------------------------------------------
@@ -325,28 +345,25 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_rtnn(args, rank, world):
+OTHER_WORKLOADS = ["radius_uniform_1e5", "knn_gmm_1e6", "knn_surface_1e7", "sph_lattice_5e7"]
+
+
+def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, headline):
+    """Times one workload: the plain grid and the learned-partition path, each with its own
+    autotuned settings, replayed from CUDA graphs; checks that both give the same neighbor
+    sets; the search kernels' roofline; the reference's CPU path on a bounded sample.
+    headline: also the per-cloud launch loop, the end-to-end host-buffer number, the
+    clock record and the full CPU sample."""
     import torch
     import rtnn_b200
-    from rtnn_b200 import build as rb
-    rb.build()
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    cfg = make_workload(args.workload, args.scale, rank)
-    ctx = rtnn_b200.Context(dev)
+    from rtnn_b200 import autotune as at
     stream = torch.cuda.current_stream()
-    ctx.set_stream(stream.cuda_stream)
-    base_tuning = ctx.tuning().as_dict()
-
+    cfg = make_workload(name, args.scale, rank)
+    ctx.set_tuning(**ctx_default_tuning(ctx))
     tp = torch.from_numpy(cfg["points"]).cuda()
     tq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).cuda()
     Q, K = cfg["n_queries"], cfg["k"]
+    N = int(len(cfg["points"]))
     out = torch.empty((Q, K), dtype=torch.int32, device="cuda")
 
     def barrier():
@@ -359,7 +376,7 @@ def run_rtnn(args, rank, world):
 
     # SPH workload: every step first moves each particle by N(0, 0.05 h), then rebuilds the
     # grid and searches (the rebuild is part of every step anyway)
-    sph = cfg["name"] == "sph_lattice_5e7"
+    sph = name == "sph_lattice_5e7"
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     noise = torch.empty_like(tp) if sph else None
 
@@ -369,33 +386,31 @@ def run_rtnn(args, rank, world):
             tp.add_(noise)
         plan.execute(tp, tq, out)
 
-    def timed(plan, steps, warmup, clocks=None):
-        for _ in range(warmup):
+    def timed(plan, n_steps, n_warm, clocks=None):
+        for _ in range(n_warm):
             step(plan)
         barrier()
         if clocks:
             clocks.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(steps):
+        for _ in range(n_steps):
             step(plan)
         e1.record(stream)
         barrier()
         ck = clocks.stop() if clocks else None
-        return max_over_ranks(e0.elapsed_time(e1) / steps), ck
+        return max_over_ranks(e0.elapsed_time(e1) / n_steps), ck
 
     common = dict(mode=cfg["mode"], radius=cfg["radius"], k=K)
-    from rtnn_b200 import autotune as at
     wl_args = (tp, cfg["offsets"], tq, cfg["qoffsets"])
+    base_tuning = ctx.tuning().as_dict()
 
     # the plain grid search (full radius for every query), with its own best tuning
-    plain_ms, plain_tuning, result_plain = None, None, None
-    if not args.no_plain:
-        plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, presets=at.GRID_PRESETS,
-                                   use_cache=False, **common)
-        plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
-        plain_ms, _ = timed(plain, args.steps, max(1, args.warmup // 2))
-        plain.close()
+    plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, presets=at.GRID_PRESETS,
+                               use_cache=False, **common)
+    plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
+    plain_ms, _ = timed(plain, steps, max(1, warmup // 2))
+    plain.close()
 
     # learned partition: for each cell-size preset the width model is trained on clouds of
     # other seeds at that grid and the margin tuned; the best preset is then tuned further
@@ -403,25 +418,24 @@ def run_rtnn(args, rank, world):
     learned_tuning, model_info = at.autotune_learned(
         ctx, *wl_args, train=lambda c: train_model(c, cfg, args.scale, rank), **common)
     learned = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=True, **common)
-    ms_learned, clocks = timed(learned, args.steps, args.warmup, ClockSampler(dev))
+    ms_learned, clocks = timed(learned, steps, warmup, ClockSampler(dev) if headline else None)
     st = rtnn_b200.Stats()
     learned.execute(tp, tq, out, stats=st)
     launches_per_step = st.n_launches
     fallback = st.n_fallback
     learned.close()
-    identical = None
-    if not args.no_plain:   # same positions, plain vs learned: identical neighbor sets
-        result_learned = _row_sets(out)
-        check = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=False, **common)
-        check.execute(tp, tq, out)
-        check.close()
-        identical = bool(torch.equal(_row_sets(out), result_learned))
-        del result_learned
+    # same positions, plain vs learned: identical neighbor sets
+    result_learned = _row_sets(out)
+    check = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=False, **common)
+    check.execute(tp, tq, out)
+    check.close()
+    identical = bool(torch.equal(_row_sets(out), result_learned))
+    del result_learned
 
     # batched vs a per-cloud launch loop (one rtnn_search per cloud, same flags/tuning)
     loop_ms = None
     n_clouds = int(len(cfg["offsets"]) - 1)
-    if n_clouds > 1:
+    if headline and n_clouds > 1:
         off = cfg["offsets"]
         qoff = cfg["qoffsets"]
 
@@ -441,10 +455,10 @@ def run_rtnn(args, rank, world):
         barrier()
         loop_ms = max_over_ranks(e0.elapsed_time(e1))
 
-    # dominant kernel (search, both passes) timed with the library's events on `stream`
+    # dominant kernels (search, all passes) timed with the library's events on `stream`
     nog = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=False, **common)
     ms_search, ms_build, ms_part, ms_fb = [], [], [], []
-    for _ in range(max(3, args.steps)):
+    for _ in range(max(3, steps)):
         s2 = rtnn_b200.Stats()
         nog.execute(tp, tq, out, stats=s2)
         ms_search.append(s2.ms_search)
@@ -453,33 +467,17 @@ def run_rtnn(args, rank, world):
         ms_part.append(s2.ms_partition)
     nog.close()
     ms_s = statistics.mean(ms_search)
-    N = int(len(cfg["points"]))
     alg_bytes = 16 * Q + 16 * N + 4 * Q * K    # sorted queries + sorted points read once, rows written
     pk, pk_src = peaks()
     achieved = alg_bytes / (ms_s * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
-                "traffic": (round(TRAFFIC_PER_QUERY[args.workload] * Q)
-                            if args.workload in TRAFFIC_PER_QUERY else None),
-                "traffic_scope": "main search pass, ncu at scale 0.1 scaled by queries",
                 "kernel": "k_search (all passes)", "peak_source": pk_src,
                 "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": round(ms_s, 4)}
     ms_main = ms_s - statistics.mean(ms_fb)
-    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
-    if args.workload in INST_PER_QUERY and mhz and ms_main > 0:
-        sms = torch.cuda.get_device_properties(dev).multi_processor_count
-        ach = INST_PER_QUERY[args.workload] * Q / (ms_main * 1e-3)
-        peak = sms * 4 * float(mhz) * 1e6   # one warp instruction per scheduler per cycle
-        roofline["issue"] = {
-            "warp_inst_per_query": INST_PER_QUERY[args.workload],
-            "achieved": round(ach / 1e12, 4), "peak": round(peak / 1e12, 4),
-            "unit": "T warp-inst/s", "frac": round(ach / peak, 3), "ms_first_pass": round(ms_main, 4),
-            "scope": "first search pass (k_search): instructions per query from ncu at scale "
-                     "0.1, time from the library's CUDA events, peak = SMs x 4 schedulers x "
-                     "median sampled SM clock"}
 
     e2e = None
-    if not args.no_e2e:
+    if headline and not args.no_e2e:
         hp = torch.from_numpy(cfg["points"]).pin_memory()
         hq = None if cfg["queries"] is None else torch.from_numpy(cfg["queries"]).pin_memory()
         ho = torch.empty((Q, K), dtype=torch.int32).pin_memory()
@@ -488,17 +486,101 @@ def run_rtnn(args, rank, world):
         ctx.search_batched(hp_np, cfg["offsets"], hq_np, cfg["qoffsets"], learned=True, out=ho_np, **common)
         barrier()
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(steps):
             ctx.search_batched(hp_np, cfg["offsets"], hq_np, cfg["qoffsets"], learned=True,
                                out=ho_np, **common)
-        dt = max_over_ranks((time.perf_counter() - t0) / args.steps)
+        dt = max_over_ranks((time.perf_counter() - t0) / steps)
         h2d = 12 * N + (0 if hq is None else 12 * Q)
         e2e = {"value": world * Q / dt, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": 4 * Q * K, "ms_per_step": round(dt * 1e3, 3)}
 
     cpu = None
     if rank == 0 and world == 1:
-        cpu = cpu_reference_sample(cfg, args.cpu_seconds, os.cpu_count() or 1)
+        cpu = cpu_reference_sample(cfg, args.cpu_seconds if headline else args.cpu_seconds / 3,
+                                   os.cpu_count() or 1)
+    del out, tp, tq
+    torch.cuda.empty_cache()
+    return {"cfg": cfg, "Q": Q, "N": N, "K": K, "plain_ms": plain_ms, "ms_learned": ms_learned,
+            "identical": identical, "fallback": int(fallback), "loop_ms": loop_ms,
+            "stage_ms": {"build": round(statistics.mean(ms_build), 3),
+                         "partition": round(statistics.mean(ms_part), 3), "search": round(ms_s, 3)},
+            "ms_main": ms_main, "model": model_info,
+            "tuning": {"learned": learned_tuning, "plain": plain_tuning},
+            "roofline": roofline, "cpu": cpu, "e2e": e2e, "launches": launches_per_step,
+            "clocks": clocks}
+
+
+def ctx_default_tuning(ctx):
+    """The tuning a fresh context starts from (each workload autotunes from there)."""
+    import rtnn_b200
+    fresh = rtnn_b200.Context(ctx.device)
+    t = fresh.tuning().as_dict()
+    fresh.close()
+    return t
+
+
+def run_rtnn(args, rank, world):
+    import torch
+    import rtnn_b200
+    from rtnn_b200 import build as rb
+    rb.build()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ctx = rtnn_b200.Context(dev)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+
+    m = measure_workload(ctx, args.workload, args, rank, world, dist, dev, args.steps,
+                         args.warmup, headline=True)
+    Q, N, K, cfg = m["Q"], m["N"], m["K"], m["cfg"]
+    ms_learned, plain_ms, loop_ms = m["ms_learned"], m["plain_ms"], m["loop_ms"]
+    roofline = m["roofline"]
+    roofline.update({"traffic": (round(TRAFFIC_PER_QUERY[args.workload] * Q)
+                                 if args.workload in TRAFFIC_PER_QUERY else None),
+                     "traffic_scope": "main search pass, ncu at scale 0.1 scaled by queries"})
+    mhz = (m["clocks"] or {}).get("sm_mhz") or (m["clocks"] or {}).get("sm_max_mhz")
+    if args.workload in INST_PER_QUERY and mhz and m["ms_main"] > 0:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        ach = INST_PER_QUERY[args.workload] * Q / (m["ms_main"] * 1e-3)
+        peak = sms * 4 * float(mhz) * 1e6   # one warp instruction per scheduler per cycle
+        roofline["issue"] = {
+            "warp_inst_per_query": INST_PER_QUERY[args.workload],
+            "achieved": round(ach / 1e12, 4), "peak": round(peak / 1e12, 4),
+            "unit": "T warp-inst/s", "frac": round(ach / peak, 3),
+            "ms_first_pass": round(m["ms_main"], 4),
+            "scope": "first search pass (k_search): instructions per query from ncu at scale "
+                     "0.1, time from the library's CUDA events, peak = SMs x 4 schedulers x "
+                     "median sampled SM clock"}
+    if args.workload in KERNEL_PROFILE:
+        roofline["kernels"] = kernel_rooflines(args.workload)
+
+    others = {}
+    if not args.no_other_workloads:
+        for name in OTHER_WORKLOADS:
+            if name == args.workload:
+                continue
+            o = measure_workload(ctx, name, args, rank, world, dist, dev,
+                                 min(args.steps, 5), max(3, min(args.warmup, 3)), headline=False)
+            oq = o["Q"]
+            best_ms = min(o["ms_learned"], o["plain_ms"])
+            others[name] = {
+                "value": world * oq / (o["ms_learned"] * 1e-3), "unit": "queries/s",
+                "ms_per_step": round(o["ms_learned"], 4),
+                "plain_value": world * oq / (o["plain_ms"] * 1e-3),
+                "learned_over_plain": o["plain_ms"] / o["ms_learned"],
+                "best_path": "learned" if o["ms_learned"] <= o["plain_ms"] else "plain",
+                "best_value": world * oq / (best_ms * 1e-3),
+                "identical_sets": o["identical"], "fallback_queries": o["fallback"],
+                "config": {"mode": o["cfg"]["mode"], "radius": o["cfg"]["radius"], "k": o["K"],
+                           "n_points": o["N"], "n_queries": oq},
+                "stage_ms": o["stage_ms"], "roofline": {"frac": o["roofline"]["frac"],
+                                                        "achieved": o["roofline"]["achieved"],
+                                                        "unit": "GB/s", "kernel": "k_search (all passes)"},
+                "cpu_baseline": o["cpu"], "tuning": o["tuning"], "steps": min(args.steps, 5)}
 
     value = world * Q / (ms_learned * 1e-3)
     line = {"metric": "queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
@@ -512,14 +594,13 @@ def run_rtnn(args, rank, world):
                        "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
             "per_cloud_loop_value": None if loop_ms is None else world * Q / (loop_ms * 1e-3),
             "batched_over_loop": None if loop_ms is None else loop_ms / ms_learned,
-            "plain_value": None if plain_ms is None else world * Q / (plain_ms * 1e-3),
-            "learned_over_plain": None if plain_ms is None else plain_ms / ms_learned,
-            "identical_sets": identical, "fallback_queries": int(fallback),
-            "stage_ms": {"build": round(statistics.mean(ms_build), 3),
-                         "partition": round(statistics.mean(ms_part), 3), "search": round(ms_s, 3)},
-            "model": model_info, "tuning": {"learned": learned_tuning, "plain": plain_tuning},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(launches_per_step * args.steps), "clocks": clocks}
+            "plain_value": world * Q / (plain_ms * 1e-3),
+            "learned_over_plain": plain_ms / ms_learned,
+            "identical_sets": m["identical"], "fallback_queries": m["fallback"],
+            "stage_ms": m["stage_ms"], "model": m["model"], "tuning": m["tuning"],
+            "roofline": roofline, "cpu_baseline": m["cpu"], "e2e": m["e2e"],
+            "gpu_launches": int(m["launches"] * args.steps), "clocks": m["clocks"],
+            "other_workloads": others}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -71,6 +71,13 @@ typedef enum rtnn_mode {
                                            sorts the queries on every run, sort.cpp:393-498,
                                            751-797); rows stay exact, only tile coherence can
                                            age. See rtnn_plan_resort. */
+#define RTNN_FLAG_REF_LAYOUT      0x80u /* rtnn_search / rtnn_search_batched: the output in the
+                                           engine's own order, as the reference returns it
+                                           (sort.cpp:378-386,612,626; search.cpp:43-53): row j
+                                           belongs to the j-th query in the search's sorted
+                                           order and every entry is a position in the engine's
+                                           cell-sorted copy of the points. rtnn_layout gives the
+                                           two permutations that map them back. */
 
 /* Per-call statistics (all optional to read). Times are device times measured with
  * CUDA events on the context stream (graph replays report ms_total only). */
@@ -113,6 +120,12 @@ rtnn_status rtnn_set_stream(rtnn_ctx* ctx, void* stream);
 
 /* Returns 1 when `k` is accepted by the searches, else 0. */
 int rtnn_k_supported(uint32_t k);
+
+/* Returns 1 when the searches have kernels with this K compiled in (the reference compiles
+ * its one K into each build, src/optixNSearch/CMakeLists.txt:58-61, camera.cu:66-72; here a
+ * fixed set: 5, 8, 16, 32, 50 and 64), else 0. Other K up to RTNN_MAX_K run kernels that
+ * take K at run time, with the same results. */
+int rtnn_k_compiled(uint32_t k);
 
 /* Version string of the library. */
 const char* rtnn_version(void);
@@ -198,6 +211,27 @@ typedef struct rtnn_tuning {
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);
 rtnn_status rtnn_set_tuning(rtnn_ctx* ctx, const rtnn_tuning* tuning);
 
+/* The order of the last successful rtnn_search / rtnn_search_batched on this context (the
+ * reference keeps the same two orders: its points sorted in place, sort.cpp:612,626, and
+ * the per-partition query arrays h_actQs, sort.cpp:378-386). point_order[i] = caller index
+ * of the i-th point of the cell-sorted copy; query_order[j] = caller index of the query of
+ * the j-th row in RTNN_FLAG_REF_LAYOUT output. So a reference-layout row j maps back as
+ * caller_row[query_order[j]][s] = point_order[row[j][s]] (-1 stays -1). Either pointer may
+ * be NULL; n_points / n_queries must equal the last search's. Host buffers unless flags
+ * holds RTNN_FLAG_DEVICE_POINTERS. Unavailable after a host-buffer batch that ran in
+ * sub-batches (a large result without RTNN_FLAG_REF_LAYOUT). */
+rtnn_status rtnn_layout(rtnn_ctx* ctx, uint32_t* point_order, uint64_t n_points,
+                        uint32_t* query_order, uint64_t n_queries, uint32_t flags);
+
+/* The library's LSD radix sort on its own (replaces thrust::sort_by_key,
+ * src/optixNSearch/thrust_helper.cu:13-43, which the reference calls at sort.cpp:415,
+ * 487-488 and 612; here it orders the queries). Sorts n (key, value) pairs in place on the
+ * device by the low key_bits bits of each key, stably (equal keys keep their input order).
+ * d_keys: n keys of key_bytes (4 or 8) bytes; d_values: n uint32 values moved with their
+ * keys. Device pointers, ordered on the context's stream; returns when done. */
+rtnn_status rtnn_sort_pairs(rtnn_ctx* ctx, void* d_keys, uint32_t key_bytes, uint32_t* d_values,
+                            uint64_t n, uint32_t key_bits);
+
 /* Failure-detection self-test (no counterpart in the reference, which has no device-side
  * waits): runs the decoupled look-back scan with a predecessor tile that is never
  * published, so its bounded wait (about a second) gives up. Returns
@@ -212,13 +246,19 @@ rtnn_status rtnn_selftest_wait_timeout(rtnn_ctx* ctx);
  * cudaMalloc, cudaFree or other allocation, and needs no context.
  * Plain (unpartitioned) radius or KNN search, the same rows as rtnn_search with flags 0.
  * Device pointers only; `stream` is a cudaStream_t (NULL: the legacy default stream); the
- * call returns after the search has finished. Its scratch is one fixed array of
+ * call returns after the search has finished. While another thread captures a CUDA graph
+ * in global mode, pass a stream created with cudaStreamNonBlocking: the legacy default
+ * stream waits on every blocking stream, so work on it would break that capture.
+ * d_queries == NULL searches the points themselves: n_queries is then ignored and the
+ * output has n_points rows. Its scratch is one fixed array of
  * RTNN_NOALLOC_SCRATCH_BYTES in device memory, held by every GPU that loads the library
  * until the process exits, and shared by all calls: calls whose work overlaps on the GPU
  * race and must be serialised by the caller. Limits: at most RTNN_NOALLOC_MAX_POINTS points
  * and RTNN_NOALLOC_MAX_QUERIES queries (RTNN_ERR_INVALID_ARGUMENT otherwise). The first call
  * on a device looks up the array's device address and should come before any stream
- * capture. errbuf (optional, errlen bytes) receives a message when the call fails. */
+ * capture; that address is kept for the life of the process, so cudaDeviceReset after the
+ * first call on a device is not supported. errbuf (optional, errlen bytes) receives a
+ * message when the call fails. */
 #define RTNN_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define RTNN_NOALLOC_MAX_POINTS (1u << 18)
 #define RTNN_NOALLOC_MAX_QUERIES (1u << 18)

@@ -4,12 +4,15 @@
  * The reference picks each partition's launch radius with an analytic rule: grow a box
  * of cells until it holds K+1 points (calcSearchSize, src/optixNSearch/grid.cu:84-211)
  * and take the equal-volume sphere radius of that box (radiusFromMegacell,
- * sort.cpp:262-269; autoBatchingKNN, sort.cpp:271-320). Here a small MLP (6 -> 32 -> 32
- * -> 1, ReLU) reads a bucket's occupancy histogram (points in cell shells 0, 1, 2
- * around the query's cell), its extent (cell / r) and K, and predicts
- * log(K-th neighbor distance / cell). The search width is margin * cell * exp(pred).
- * Results never depend on the model: a query that finds fewer than K neighbors inside
- * its width is re-searched at the full radius.
+ * sort.cpp:262-269; autoBatchingKNN, sort.cpp:271-320). Here the bucket is the search's
+ * tile of 32 consecutive (Hilbert-ordered) queries, and a small MLP (6 -> 32 -> 32 -> 1,
+ * ReLU) reads the bucket's occupancy histogram (log1p of the points in cell shells 0, 1,
+ * 2 around the cell of the tile's box centre, and log(K+1) - log1p(N2)), log(cell / r)
+ * and its extent (log1p of the tile box's longest side in cells), and predicts
+ * log(largest K-th neighbor distance of the tile's queries / cell). The search kernel
+ * evaluates it once per tile and searches the tile at margin * cell * exp(pred), at most
+ * r. Results never depend on the model: a query that finds fewer than K neighbors inside
+ * its width is searched again wider, finally at the full radius.
  *
  * The network is trained on the GPU by hand-written kernels (forward, backward, Adam)
  * on exact K-th distances produced by the plain search. All pointers are device
@@ -35,12 +38,16 @@ uint32_t rtnn_model_size(void);
 rtnn_status rtnn_model_set(rtnn_ctx* ctx, const float* params, uint32_t n);
 rtnn_status rtnn_model_get(rtnn_ctx* ctx, float* params, uint32_t n);
 
-/* Runs the plain search (sorted rows) on one cloud and writes, per query, its six
- * bucket features (d_feats[q][6]) and the target log(K-th distance / cell)
- * (d_target[q]); a query with fewer than K neighbors within r gets log(1.5 r / cell). */
+/* Runs the plain search (sorted rows) on one cloud and writes one training sample per
+ * tile of that search (the buckets the learned search forms on the same data): the six
+ * bucket features (d_feats[t][6]) and the target log(largest K-th neighbor distance of the
+ * tile's queries / cell) (d_target[t]); queries with fewer than K neighbors within r do not
+ * count, and a tile of only such queries gets log(1.5 r / cell). *n_samples receives the
+ * number of tiles, ceil(n_queries / 32); buffers sized for that many samples suffice. */
 rtnn_status rtnn_collect_training(rtnn_ctx* ctx, const float* d_points, uint64_t n_points,
                                   const float* d_queries, uint64_t n_queries, rtnn_mode mode,
-                                  float radius, uint32_t k, float* d_feats, float* d_target);
+                                  float radius, uint32_t k, float* d_feats, float* d_target,
+                                  uint64_t* n_samples);
 
 /* Trains the context's model from scratch with Adam (mean squared error on the
  * normalised target), `batch` samples per step, in the given sample order.
@@ -49,9 +56,10 @@ rtnn_status rtnn_model_train(rtnn_ctx* ctx, const float* d_feats, const float* d
                              uint64_t n, uint32_t epochs, uint32_t batch, float lr,
                              uint64_t seed, float* loss_per_epoch);
 
-/* The search width of every query under the partition (analytic, or the loaded model
- * with RTNN_FLAG_LEARNED), in query order; d_widths[q] >= radius means the full radius.
- * Runs the whole partitioned search of one cloud (rows discarded). */
+/* The first-pass search width of every query under the partition (analytic, per query;
+ * or, with RTNN_FLAG_LEARNED, the loaded model's width of the query's tile), in query
+ * order; d_widths[q] >= radius means the full radius. Runs the whole partitioned search
+ * of one cloud (rows discarded). */
 rtnn_status rtnn_query_widths(rtnn_ctx* ctx, const float* d_points, uint64_t n_points,
                               const float* d_queries, uint64_t n_queries, rtnn_mode mode,
                               float radius, uint32_t k, uint32_t flags, float* d_widths);

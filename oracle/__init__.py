@@ -173,9 +173,10 @@ def ref_available():
         os.path.exists(os.path.join(REF_DIR, "libref.so"))
 
 
-def refcheck(points, queries, rows, mode, r, k, q_begin=None, q_end=None):
+def refcheck(points, queries, rows, mode, r, k, q_begin=None, q_end=None, procs=1):
     """Runs the reference's sanityCheckRadius / sanityCheckKNN on rows. Returns
-    (passed, output)."""
+    (passed, output). procs > 1 (KNN): the query range is split over that many
+    processes, each running the reference's check on its part."""
     exe = os.path.join(REF_DIR, "refcheck")
     with tempfile.TemporaryDirectory() as d:
         pf, qf, rf = (os.path.join(d, n) for n in ("p.bin", "q.bin", "r.bin"))
@@ -185,8 +186,19 @@ def refcheck(points, queries, rows, mode, r, k, q_begin=None, q_end=None):
         else:
             _f32(queries).tofile(qf)
             qarg = qf
-        np.ascontiguousarray(rows, dtype=np.int32).tofile(rf)
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        rows.tofile(rf)
         cmd = [exe, pf, qarg, rf, "knn" if _mode(mode) else "radius", repr(float(r)), str(int(k))]
+        if _mode(mode) and procs > 1:
+            lo = 0 if q_begin is None else int(q_begin)
+            hi = rows.shape[0] if q_end is None else int(q_end)
+            cuts = np.linspace(lo, hi, procs + 1).astype(int)
+            ps = [subprocess.Popen(cmd + [str(cuts[i]), str(cuts[i + 1])], stdout=subprocess.PIPE,
+                                   stderr=subprocess.STDOUT, text=True)
+                  for i in range(procs) if cuts[i + 1] > cuts[i]]
+            outs = [pp.communicate()[0] for pp in ps]
+            ok = all(pp.returncode == 0 for pp in ps) and all("REFCHECK OK" in o for o in outs)
+            return ok, "".join(outs)
         if q_begin is not None:
             cmd += [str(q_begin), str(q_end)]
         res = subprocess.run(cmd, capture_output=True, text=True)

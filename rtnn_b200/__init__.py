@@ -15,7 +15,8 @@ import numpy as np
 
 __all__ = ["RtnnError", "Stats", "Tuning", "Context", "Plan", "search", "search_batched",
            "RADIUS", "KNN", "FLAG_DEVICE_POINTERS", "FLAG_PARTITION", "FLAG_LEARNED",
-           "FLAG_SORTED_ROWS", "FLAG_LOCAL_INDICES", "FLAG_ANY_K", "FLAG_KEEP_ORDER", "MAX_K",
+           "FLAG_SORTED_ROWS", "FLAG_LOCAL_INDICES", "FLAG_ANY_K", "FLAG_KEEP_ORDER",
+           "FLAG_REF_LAYOUT", "MAX_K", "from_ref_layout",
            "library_path", "load_library"]
 
 RADIUS = 0
@@ -27,6 +28,7 @@ FLAG_SORTED_ROWS = 0x8
 FLAG_LOCAL_INDICES = 0x10
 FLAG_ANY_K = 0x20
 FLAG_KEEP_ORDER = 0x40
+FLAG_REF_LAYOUT = 0x80
 MAX_K = 128
 MODEL_FEATURES = 6   # RTNN_MODEL_FEATURES
 MODEL_NORM_PARAMS = 2 * MODEL_FEATURES + 2   # RTNN_MODEL_NORM_PARAMS
@@ -93,6 +95,7 @@ _I = ctypes.c_int
 _SIGS = {
     "rtnn_version": (ctypes.c_char_p, []),
     "rtnn_k_supported": (_I, [_U32]),
+    "rtnn_k_compiled": (_I, [_U32]),
     "rtnn_create": (_I, [ctypes.POINTER(_P), _I]),
     "rtnn_destroy": (_I, [_P]),
     "rtnn_last_error": (ctypes.c_char_p, [_P]),
@@ -109,7 +112,8 @@ _SIGS = {
     "rtnn_model_size": (_U32, []),
     "rtnn_model_set": (_I, [_P, _P, _U32]),
     "rtnn_model_get": (_I, [_P, _P, _U32]),
-    "rtnn_collect_training": (_I, [_P, _P, _U64, _P, _U64, _I, _F, _U32, _P, _P]),
+    "rtnn_collect_training": (_I, [_P, _P, _U64, _P, _U64, _I, _F, _U32, _P, _P,
+                                   ctypes.POINTER(_U64)]),
     "rtnn_model_train": (_I, [_P, _P, _P, _U64, _U32, _U32, _F, _U64, _P]),
     "rtnn_query_widths": (_I, [_P, _P, _U64, _P, _U64, _I, _F, _U32, _U32, _P]),
     "rtnn_mlp_loss_grad": (_I, [_P, _P, _P, _P, _U32, _P, _P]),
@@ -118,6 +122,8 @@ _SIGS = {
     "rtnn_search_noalloc": (_I, [_P, _U32, _P, _U32, _I, _F, _U32, _P, _P, ctypes.c_char_p,
                                  ctypes.c_size_t]),
     "rtnn_selftest_wait_timeout": (_I, [_P]),
+    "rtnn_sort_pairs": (_I, [_P, _P, _U32, _P, _U64, _U32]),
+    "rtnn_layout": (_I, [_P, _P, _U64, _P, _U64, _U32]),
 }
 
 
@@ -204,19 +210,22 @@ class Context:
 
     # -- single cloud -------------------------------------------------------------------
     def search(self, points, queries=None, mode="radius", radius=2.0, k=50, partition=False,
-               learned=False, sorted_rows=False, any_k=False, out=None, stats=None):
+               learned=False, sorted_rows=False, any_k=False, ref_layout=False, out=None,
+               stats=None):
         """Neighbors of every query: [Q, k] int32, -1 in unused slots.
 
         points / queries: numpy [n, 3] float32 (host; copies happen inside the call) or
         CUDA torch tensors [n, 3] float32 (device; `out` may be a preallocated CUDA
         int32 tensor [Q, k]). mode: "radius" (self included) or "knn" (0 < d < r^2).
         any_k: any K qualifying points (the reference's radius semantics) instead of the
-        K nearest.
+        K nearest. ref_layout: rows in the engine's sorted query order holding positions in
+        its sorted point copy (the reference's layout); layout() maps them back.
         """
         lib = load_library()
         m = _mode(mode)
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
-                 (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_ANY_K if any_k else 0))
+                 (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_ANY_K if any_k else 0) |
+                 (FLAG_REF_LAYOUT if ref_layout else 0))
         st = stats if stats is not None else Stats()
         if _is_torch(points):
             import torch
@@ -246,7 +255,8 @@ class Context:
     # -- many clouds --------------------------------------------------------------------
     def search_batched(self, points, point_offsets, queries=None, query_offsets=None,
                        mode="knn", radius=0.2, k=32, partition=False, learned=False,
-                       sorted_rows=False, local_indices=False, any_k=False, out=None, stats=None):
+                       sorted_rows=False, local_indices=False, any_k=False, ref_layout=False,
+                       out=None, stats=None):
         """Many independent clouds in one launch; offsets have n_clouds + 1 entries."""
         lib = load_library()
         po = np.ascontiguousarray(np.asarray(point_offsets, dtype=np.uint64))
@@ -255,7 +265,7 @@ class Context:
         n_clouds = po.shape[0] - 1
         flags = ((FLAG_PARTITION if partition else 0) | (FLAG_LEARNED if learned else 0) |
                  (FLAG_SORTED_ROWS if sorted_rows else 0) | (FLAG_LOCAL_INDICES if local_indices else 0) |
-                 (FLAG_ANY_K if any_k else 0))
+                 (FLAG_ANY_K if any_k else 0) | (FLAG_REF_LAYOUT if ref_layout else 0))
         st = stats if stats is not None else Stats()
         nq = int(po[-1]) if queries is None else int(qo[-1])
         if _is_torch(points):
@@ -302,16 +312,19 @@ class Context:
         return p
 
     def collect_training(self, points, queries=None, mode="knn", radius=2.0, k=16):
-        """(features [Q, 6], targets [Q]) as CUDA tensors from one plain search."""
+        """(features [T, 6], targets [T]) as CUDA tensors, one sample per 32-query tile of
+        one plain search (rtnn_collect_training)."""
         import torch
         nq = points.shape[0] if queries is None else queries.shape[0]
-        feats = torch.empty((nq, MODEL_FEATURES), dtype=torch.float32, device=points.device)
-        tgt = torch.empty((nq,), dtype=torch.float32, device=points.device)
+        cap = max(1, (nq + 31) // 32)
+        feats = torch.empty((cap, MODEL_FEATURES), dtype=torch.float32, device=points.device)
+        tgt = torch.empty((cap,), dtype=torch.float32, device=points.device)
+        n = _U64(0)
         self._check(load_library().rtnn_collect_training(
             self._h, _P(points.data_ptr()), points.shape[0],
             _P(queries.data_ptr()) if queries is not None else None, nq, _mode(mode),
-            float(radius), int(k), _P(feats.data_ptr()), _P(tgt.data_ptr())))
-        return feats, tgt
+            float(radius), int(k), _P(feats.data_ptr()), _P(tgt.data_ptr()), ctypes.byref(n)))
+        return feats[:n.value], tgt[:n.value]
 
     def train_model(self, feats, target, epochs=20, batch=8192, lr=3e-3, seed=0):
         """Trains the width model on the GPU; returns the per-epoch mean loss."""
@@ -348,6 +361,32 @@ class Context:
         self._check(load_library().rtnn_mlp_forward(
             self._h, _P(params.data_ptr()), _P(feats.data_ptr()), feats.shape[0], _P(y.data_ptr())))
         return y
+
+    def layout(self, n_points, n_queries, device=False):
+        """(point_order, query_order) of the last search (rtnn_layout): numpy uint32 arrays,
+        or CUDA int32 tensors with device=True."""
+        lib = load_library()
+        if device:
+            import torch
+            po = torch.empty(n_points, dtype=torch.int32, device=f"cuda:{self.device}")
+            qo = torch.empty(n_queries, dtype=torch.int32, device=f"cuda:{self.device}")
+            self._check(lib.rtnn_layout(self._h, _P(po.data_ptr()), n_points, _P(qo.data_ptr()),
+                                        n_queries, FLAG_DEVICE_POINTERS))
+            return po, qo
+        po = np.empty(n_points, dtype=np.uint32)
+        qo = np.empty(n_queries, dtype=np.uint32)
+        self._check(lib.rtnn_layout(self._h, po.ctypes.data_as(_P), n_points,
+                                    qo.ctypes.data_as(_P), n_queries, 0))
+        return po, qo
+
+    def sort_pairs(self, keys, values, key_bits=None):
+        """Sorts CUDA tensors keys (int32/uint32 or int64/uint64) and values (int32, the same
+        length) in place by the low key_bits bits of the keys, stably (rtnn_sort_pairs)."""
+        kb = keys.element_size()
+        bits = 8 * kb if key_bits is None else int(key_bits)
+        self._check(load_library().rtnn_sort_pairs(self._h, _P(keys.data_ptr()), kb,
+                                                   _P(values.data_ptr()), keys.numel(), bits))
+        return keys, values
 
     def mlp_adam_step(self, params, grad, m, v, lr, step, grad_scale):
         self._check(load_library().rtnn_mlp_adam_step(
@@ -402,6 +441,18 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def from_ref_layout(rows, point_order, query_order):
+    """Rows of a reference-layout search (RTNN_FLAG_REF_LAYOUT) in the caller's layout:
+    row query_order[j] = point_order[rows[j]], -1 kept (host numpy)."""
+    rows = np.asarray(rows)
+    po = np.asarray(point_order).astype(np.int64)
+    qo = np.asarray(query_order).astype(np.int64)
+    out = np.full_like(rows, -1)
+    valid = rows >= 0
+    out[qo] = np.where(valid, po[np.where(valid, rows, 0)], -1).astype(rows.dtype)
+    return out
 
 
 def _mode(mode):

@@ -46,9 +46,10 @@ GRID_PRESETS = [
     {"cell_ratio": 0.125, "min_cell_ratio": 0.01, "points_per_cell": 0.125, "query_warps": 2},
     {"cell_ratio": 1.0, "min_cell_ratio": 0.0625, "points_per_cell": 4.0, "query_warps": 0},
 ]
+# the learned widths are per tile (the search's bucket), so the analytic partition's
+# width buckets (buckets_per_halving) do not apply
 LEARNED_KNOBS = [
-    ("buckets_per_halving", [0.0, 0.5, 1.0, 2.0]),
-    ("width_margin", [1.0, 1.08, 1.15, 1.25, 1.4]),
+    ("width_margin", [0.9, 1.0, 1.08, 1.15, 1.25]),
     ("fallback_passes", [2, 4, 6]),
 ]
 

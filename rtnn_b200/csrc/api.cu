@@ -56,13 +56,13 @@ void release(DevBuf& b) {
 struct Workspace {
   DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth,
       qwidth_in, fbflag, fbnextw, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters,
-      in_pts, in_qs, out, feats, cellsz, kth;
+      in_pts, in_qs, out, kth, ppos;
   bool order_in1 = false;   // the last query sort left its permutation in vals1 (else vals0)
   void release_all() {
     for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
                       &vals1, &sq, &qwidth, &qwidth_in, &fbflag, &fbnextw, &fbpos[0], &fbpos[1],
                       &fbcloud[0], &fbcloud[1], &fbwidth[0], &fbwidth[1], &hist, &scan_state, &counters,
-                      &in_pts, &in_qs, &out, &feats, &cellsz, &kth})
+                      &in_pts, &in_qs, &out, &kth, &ppos})
       release(*b);
   }
 };
@@ -115,6 +115,9 @@ struct rtnn_ctx {
   cudaStream_t copy = nullptr;
   cudaEvent_t sub_ev[8][5] = {};
   DevBuf sub_ctr;
+  // the order of the last search in ws (rtnn_layout): valid after a one-batch search
+  bool layout_valid = false;
+  uint64_t layout_n = 0, layout_q = 0;
 };
 
 struct rtnn_plan {
@@ -160,9 +163,13 @@ rtnn_status check_args(rtnn_ctx* c, uint64_t N, uint64_t Q, float radius, uint32
   if (N >= (1ull << 31) || Q >= (1ull << 31))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 points and queries");
   const uint32_t known = RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED |
-                         RTNN_FLAG_SORTED_ROWS | RTNN_FLAG_LOCAL_INDICES | RTNN_FLAG_ANY_K;
+                         RTNN_FLAG_SORTED_ROWS | RTNN_FLAG_LOCAL_INDICES | RTNN_FLAG_ANY_K |
+                         RTNN_FLAG_REF_LAYOUT;
   if ((flags & RTNN_FLAG_KEEP_ORDER) && !plan)
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "RTNN_FLAG_KEEP_ORDER applies to plans only");
+  if ((flags & RTNN_FLAG_REF_LAYOUT) && plan)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT,
+                "RTNN_FLAG_REF_LAYOUT applies to rtnn_search and rtnn_search_batched only");
   if (flags & ~(known | RTNN_FLAG_KEEP_ORDER))
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "unknown flag bits");
   if ((flags & RTNN_FLAG_LEARNED) && !c->has_model)
@@ -252,8 +259,14 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
   return RTNN_OK;
 }
 
+// narrowed widths with escalation passes: the analytic partition or the learned widths
 bool partitioned(const Params& p) { return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0; }
-uint32_t level_bits_of(const Params& p) { return partitioned(p) ? 4u : 0u; }
+// a width per query before the sort (the analytic partition); the learned widths are per
+// tile, computed by the search kernel itself
+bool per_query_widths(const Params& p) {
+  return (p.flags & RTNN_FLAG_PARTITION) != 0 && (p.flags & RTNN_FLAG_LEARNED) == 0;
+}
+uint32_t level_bits_of(const Params& p) { return per_query_widths(p) ? 4u : 0u; }
 uint32_t key_bits_of(const Shapes& sh, const Params& p) { return sh.key_bits + level_bits_of(p); }
 bool key64_of(const Shapes& sh, const Params& p) { return key_bits_of(sh, p) > 32; }
 
@@ -275,9 +288,12 @@ rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& 
   RTNN_CU(ensure(ws.vals0, Q * 4), "alloc vals");
   RTNN_CU(ensure(ws.vals1, Q * 4), "alloc vals");
   RTNN_CU(ensure(ws.sq, Q * 16), "alloc sorted queries");
-  if (partitioned(pr)) {
+  if (pr.flags & RTNN_FLAG_REF_LAYOUT) RTNN_CU(ensure(ws.ppos, N * 4), "alloc point positions");
+  if (per_query_widths(pr)) {
     RTNN_CU(ensure(ws.qwidth, Q * 4), "alloc widths");
     RTNN_CU(ensure(ws.qwidth_in, Q * 4), "alloc widths");
+  }
+  if (partitioned(pr)) {
     for (int i = 0; i < 2; ++i) {
       RTNN_CU(ensure(ws.fbpos[i], Q * 4), "alloc fallback list");
       RTNN_CU(ensure(ws.fbcloud[i], Q * 4), "alloc fallback list");
@@ -307,11 +323,11 @@ CloudTables tables_of(const Workspace& ws, uint32_t n_clouds) {
 
 // Issues the whole pipeline on stream s. ev: 4 events (or nullptr) bracketing
 // build | partition | search.
-uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats, bool reuse_order = false) {
+uint32_t launches_of(const Shapes& sh, const Params& pr, bool reuse_order = false) {
   const uint32_t passes = sh.Q ? (key_bits_of(sh, pr) + 7) / 8 : 0;
   // tables, build (6), query keys + sort (skipped when a kept order is reused), gather
   uint32_t n = (sh.single ? 1 : 0) + 6 + (reuse_order ? 0 : 1 + 3 * passes) + 1;
-  if (partitioned(pr) || feats) n += 1;                      // widths
+  if (per_query_widths(pr)) n += 1;                          // analytic widths
   // search passes; each flagging pass adds a flag scan and a compaction
   n += partitioned(pr) ? 3 * fallback_passes_of(pr) + 4 : 1;
   return n;
@@ -319,8 +335,8 @@ uint32_t launches_of(const Shapes& sh, const Params& pr, bool feats, bool reuse_
 
 rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr,
                   const float* d_pts, const float* d_qs, int32_t* d_out, cudaStream_t s,
-                  cudaEvent_t* ev, float* feats_out = nullptr, float* cellsz_out = nullptr,
-                  uint32_t index_base = 0, bool reuse_order = false) {
+                  cudaEvent_t* ev, uint32_t index_base = 0, bool reuse_order = false,
+                  float* width_out = nullptr) {
   Counters* ctr = (Counters*)ws.counters.p;
   const bool knn = pr.mode == RTNN_MODE_KNN;
   const rtnn_tuning& tu = c->tuning;
@@ -344,15 +360,18 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   RTNN_CU(launch_scan_excl(cells, 0, &ctr->total_cells, 1, sh.cell_capacity + 1,
                            (uint64_t*)ws.scan_state.p, &ctr->scan_tiles[0], ctr, s),
           "scan cells");
+  const bool ref_layout = (pr.flags & RTNN_FLAG_REF_LAYOUT) != 0;
   RTNN_CU(launch_scatter(d_pts, sh.N, ap, t, sh.n_chunks, grids, cells, (uint32_t*)ws.rank.p,
-                         (float4*)ws.spts.p, ctr, s),
+                         (float4*)ws.spts.p, ctr, s, ref_layout ? (uint32_t*)ws.ppos.p : nullptr),
           "scatter");
   if (ev) RTNN_CU(cudaEventRecord(ev[1], s), "event");
 
-  // density buckets: a width per query (caller's order), then the sort key
+  // analytic density buckets: a width per query (caller's order), then the sort key
   // cloud | bucket of the width | Hilbert index, so each 32-query tile shares one width
+  // band; the learned widths come per tile from the search kernel itself
   const bool part = partitioned(pr);
-  if (part || feats_out) {
+  const bool pqw = per_query_widths(pr);
+  if (pqw) {
     WidthArgs w{};
     w.t = t;
     w.grids = grids;
@@ -366,11 +385,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     w.radius = pr.radius;
     w.need = pr.k + 1;
     w.alpha = 1.24f;   // equal-volume radius of a (2s+2)-cell cube, util.cpp:422-426
-    w.model = (pr.flags & RTNN_FLAG_LEARNED) ? (const float*)c->model.p : nullptr;
-    w.margin = tu.width_margin;
     w.qwidth = (float*)ws.qwidth_in.p;
-    w.feats = feats_out;
-    w.cellsz = cellsz_out;
     RTNN_CU(launch_widths(w, c->n_sms, s), "widths");
   }
   // reuse_order (a RTNN_FLAG_KEEP_ORDER plan after its first execute): the permutation of
@@ -379,7 +394,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   if (!reuse_order) {
     const bool key64 = key64_of(sh, pr);
     RTNN_CU(launch_query_keys(d_qs, sh.Q, aq, t, sh.n_qchunks, grids, sh.order_bits,
-                              part ? (const float*)ws.qwidth_in.p : nullptr, pr.radius,
+                              pqw ? (const float*)ws.qwidth_in.p : nullptr, pr.radius,
                               level_bits_of(pr), tu.buckets_per_halving, key64, ws.keys0.p, s),
             "query keys");
     bool in1 = false;
@@ -392,8 +407,8 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   }
   const uint32_t* order = (const uint32_t*)(ws.order_in1 ? ws.vals1.p : ws.vals0.p);
   RTNN_CU(launch_gather_queries(d_qs, order, (uint32_t)sh.Q, (float4*)ws.sq.p,
-                                part ? (const float*)ws.qwidth_in.p : nullptr,
-                                part ? (float*)ws.qwidth.p : nullptr, c->n_sms, s),
+                                pqw ? (const float*)ws.qwidth_in.p : nullptr,
+                                pqw ? (float*)ws.qwidth.p : nullptr, c->n_sms, s),
           "gather queries");
   if (ev) RTNN_CU(cudaEventRecord(ev[2], s), "event");
 
@@ -403,7 +418,10 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.cells = cells;
   a.spts = (const float4*)ws.spts.p;
   a.sq = (const float4*)ws.sq.p;
-  a.qwidth = part ? (const float*)ws.qwidth.p : nullptr;
+  a.qwidth = pqw ? (const float*)ws.qwidth.p : nullptr;
+  a.model = (pr.flags & RTNN_FLAG_LEARNED) ? (const float*)c->model.p : nullptr;
+  a.margin = tu.width_margin;
+  a.width_out = width_out;
   a.out = d_out;
   a.ctr = ctr;
   a.n_tiles = sh.n_tiles;
@@ -411,6 +429,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.r2 = pr.radius * pr.radius;
   a.k = pr.k;
   a.index_base = index_base;
+  a.ref_ppos = ref_layout ? (const uint32_t*)ws.ppos.p : nullptr;
   a.lane_walk_ratio = tu.lane_walk_ratio;
   a.gap_ratio = tu.gap_ratio;
   a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
@@ -510,7 +529,7 @@ rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& 
     stats->grid_dims[0] = (uint32_t)c->h_grid->dx;
     stats->grid_dims[1] = (uint32_t)c->h_grid->dy;
     stats->grid_dims[2] = (uint32_t)c->h_grid->dz;
-    stats->n_launches = launches_of(sh, pr, false, reuse_order);
+    stats->n_launches = launches_of(sh, pr, reuse_order);
     stats->n_loaded = h.n_loaded;
     stats->n_tested = h.n_tested;
     if (timed) {
@@ -526,10 +545,11 @@ rtnn_status read_back(rtnn_ctx* c, Workspace& ws, cudaStream_t s, const Shapes& 
 
 cudaStream_t stream_of(rtnn_ctx* c) { return c->stream ? c->stream : c->own; }
 
-// Full search with optional host staging. feats/cellsz (device) collect MLP features.
+// Full search with optional host staging. width_out (device, optional): the main-pass
+// search width of every query.
 rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const float* points,
                        const float* queries, int32_t* out, rtnn_stats* stats,
-                       float* feats = nullptr, float* cellsz = nullptr) {
+                       float* width_out = nullptr) {
   cudaStream_t s = stream_of(c);
   const bool dev = (pr.flags & RTNN_FLAG_DEVICE_POINTERS) != 0;
   const bool same = (queries == nullptr);
@@ -540,6 +560,7 @@ rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const fl
   const float* d_qs = same ? points : queries;
   int32_t* d_out = out;
   const size_t out_bytes = (size_t)sh.Q * pr.k * sizeof(int32_t);
+  c->layout_valid = false;
   if (!dev) {
     RTNN_CU(ensure(c->ws.in_pts, std::max<uint64_t>(sh.N, 1) * 12), "alloc points");
     RTNN_CU(cudaMemcpyAsync(c->ws.in_pts.p, points, sh.N * 12, cudaMemcpyHostToDevice, s), "copy points");
@@ -557,7 +578,7 @@ rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const fl
   if (sh.N == 0) {
     RTNN_CU(cudaMemsetAsync(d_out, 0xff, out_bytes, s), "fill output");
   } else {
-    st = issue(c, c->ws, sh, pr, d_pts, d_qs, d_out, s, c->ev, feats, cellsz);
+    st = issue(c, c->ws, sh, pr, d_pts, d_qs, d_out, s, c->ev, 0, false, width_out);
     if (st != RTNN_OK) return st;
   }
   if (!dev) RTNN_CU(cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, s), "copy output");
@@ -570,7 +591,13 @@ rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const fl
     }
     return RTNN_OK;
   }
-  return read_back(c, c->ws, s, sh, pr, stats, true);
+  st = read_back(c, c->ws, s, sh, pr, stats, true);
+  if (st == RTNN_OK) {
+    c->layout_valid = true;
+    c->layout_n = sh.N;
+    c->layout_q = sh.Q;
+  }
+  return st;
 }
 
 // Host buffers, many clouds: the batch runs as sub-batches of whole clouds (about equal
@@ -594,6 +621,7 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
                                    rtnn_stats* stats, uint32_t n_sub) {
   const uint64_t* qoff = queries ? query_off : point_off;
   const uint64_t N = point_off[n_clouds], Q = qoff[n_clouds];
+  c->layout_valid = false;   // the workspace ends up holding only the last sub-batch
   // cloud boundaries: sub-batch g starts at the first cloud holding query Q * g / n_sub
   std::vector<uint32_t> cut{0};
   for (uint32_t g = 1; g < n_sub; ++g) {
@@ -650,7 +678,7 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
     } else {
       const rtnn_status st = issue(c, c->ws, sh, pr, d_pts + 3 * point_off[cut[g]],
                                    d_qs + 3 * qoff[cut[g]], d_out + qoff[cut[g]] * pr.k, s,
-                                   c->sub_ev[g], nullptr, nullptr, (uint32_t)point_off[cut[g]]);
+                                   c->sub_ev[g], (uint32_t)point_off[cut[g]]);
       if (st != RTNN_OK) return st;
       RTNN_CU(cudaMemcpyAsync(d_sub + g, c->ws.counters.p, sizeof(Counters), cudaMemcpyDeviceToDevice, s),
               "save counters");
@@ -695,7 +723,7 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
       if (partitioned(pr)) stats->n_fallback += h[g].fb_count[0];
       stats->n_tiles += sh.n_tiles;
       stats->n_cells += h[g].total_cells;
-      stats->n_launches += (sh.N && sh.Q) ? launches_of(sh, pr, false) : 0;
+      stats->n_launches += (sh.N && sh.Q) ? launches_of(sh, pr) : 0;
       stats->n_loaded += h[g].n_loaded;
       stats->n_tested += h[g].n_tested;
       float t[5] = {0, 0, 0, 0, 0};
@@ -723,6 +751,8 @@ extern "C" {
 const char* rtnn_version(void) { return "rtnn_b200 0.1.0 (sm_100a)"; }
 
 int rtnn_k_supported(uint32_t k) { return (k >= 1 && k <= RTNN_MAX_K) ? 1 : 0; }
+
+int rtnn_k_compiled(uint32_t k) { return search_compiled_k(k) != 0 ? 1 : 0; }
 
 rtnn_status rtnn_create(rtnn_ctx** out, int device) {
   if (!out) return RTNN_ERR_INVALID_ARGUMENT;
@@ -843,7 +873,7 @@ rtnn_status rtnn_search_batched(rtnn_ctx* c, const float* points, const uint64_t
   const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
   st = reserve(c, c->ws, sh, pr);
   if (st != RTNN_OK) return st;
-  const uint32_t n_sub = (flags & RTNN_FLAG_DEVICE_POINTERS) || sh.N == 0
+  const uint32_t n_sub = (flags & (RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_REF_LAYOUT)) || sh.N == 0
                             ? 1u : overlap_sub_batches((uint64_t)sh.Q * k * 4, n_clouds);
   if (n_sub > 1)
     return run_batched_overlapped(c, point_offsets, n_clouds, points, queries, query_offsets, pr,
@@ -904,8 +934,7 @@ rtnn_status rtnn_plan_execute(rtnn_plan* p, const float* d_points, const float* 
   const float* d_qs = d_queries ? d_queries : d_points;
   const bool reuse = p->keep_order && p->have_order;
   if (!p->use_graph) {
-    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, c->ev, nullptr,
-                           nullptr, 0, reuse);
+    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, c->ev, 0, reuse);
     if (st != RTNN_OK) return st;
     st = read_back(c, p->ws, s, p->sh, p->pr, stats, true, reuse);
     if (st == RTNN_OK && p->keep_order) p->have_order = true;
@@ -916,8 +945,7 @@ rtnn_status rtnn_plan_execute(rtnn_plan* p, const float* d_points, const float* 
     if (p->exec[m]) { cudaGraphExecDestroy(p->exec[m]); p->exec[m] = nullptr; }
     if (p->graph[m]) { cudaGraphDestroy(p->graph[m]); p->graph[m] = nullptr; }
     RTNN_CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, nullptr, nullptr,
-                           nullptr, 0, reuse);
+    rtnn_status st = issue(c, p->ws, p->sh, p->pr, d_points, d_qs, d_out, s, nullptr, 0, reuse);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (st != RTNN_OK) { if (g) cudaGraphDestroy(g); return st; }
@@ -983,9 +1011,11 @@ rtnn_status rtnn_model_get(rtnn_ctx* c, float* params, uint32_t n) {
 
 rtnn_status rtnn_collect_training(rtnn_ctx* c, const float* d_points, uint64_t n_points,
                                   const float* d_queries, uint64_t n_queries, rtnn_mode mode,
-                                  float radius, uint32_t k, float* d_feats, float* d_target) {
-  if (!c || !d_points || !d_feats || !d_target) return RTNN_ERR_INVALID_ARGUMENT;
+                                  float radius, uint32_t k, float* d_feats, float* d_target,
+                                  uint64_t* n_samples) {
+  if (!c || !d_points || !d_feats || !d_target || !n_samples) return RTNN_ERR_INVALID_ARGUMENT;
   c->err.clear();
+  *n_samples = 0;
   if (d_queries == nullptr) n_queries = n_points;
   const uint32_t flags = RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_SORTED_ROWS;
   rtnn_status st = check_args(c, n_points, n_queries, radius, k, flags);
@@ -994,28 +1024,30 @@ rtnn_status rtnn_collect_training(rtnn_ctx* c, const float* d_points, uint64_t n
   cudaSetDevice(c->device);
   cudaStream_t s = stream_of(c);
   RTNN_CU(ensure(c->ws.out, (size_t)n_queries * k * 4), "alloc rows");
-  RTNN_CU(ensure(c->ws.cellsz, n_queries * 4), "alloc cell sizes");
   RTNN_CU(ensure(c->ws.kth, n_queries * 4), "alloc kth");
-  RTNN_CU(ensure(c->ws.qwidth_in, n_queries * 4), "alloc widths");
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
   const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
   int32_t* rows = (int32_t*)c->ws.out.p;
-  st = run_search(c, sh, pr, d_points, d_queries, rows, nullptr, d_feats, (float*)c->ws.cellsz.p);
+  // the plain search: exact rows, and the tiles (sorted queries) the learned search forms
+  st = run_search(c, sh, pr, d_points, d_queries, rows, nullptr);
   if (st != RTNN_OK) return st;
   const float* qs = d_queries ? d_queries : d_points;
   RTNN_CU(launch_kth_dist(rows, (uint32_t)n_queries, k, d_points, qs, (float*)c->ws.kth.p, s), "kth");
-  // target = log(kth / cell); queries with < K neighbors inside r get log(1.5 r / cell)
-  std::vector<float> kth(n_queries), cz(n_queries);
-  RTNN_CU(cudaMemcpyAsync(kth.data(), c->ws.kth.p, n_queries * 4, cudaMemcpyDeviceToHost, s), "copy");
-  RTNN_CU(cudaMemcpyAsync(cz.data(), c->ws.cellsz.p, n_queries * 4, cudaMemcpyDeviceToHost, s), "copy");
+  TileSampleArgs a{};
+  a.t = tables_of(c->ws, 1);
+  a.grids = (const CloudGrid*)c->ws.grids.p;
+  a.cells = (const uint32_t*)c->ws.cells.p;
+  a.total_cells = &((const Counters*)c->ws.counters.p)->total_cells;
+  a.sq = (const float4*)c->ws.sq.p;
+  a.kth = (const float*)c->ws.kth.p;
+  a.n_tiles = sh.n_tiles;
+  a.need = k + 1;
+  a.radius = radius;
+  a.feats = d_feats;
+  a.target = d_target;
+  RTNN_CU(launch_tile_samples(a, c->n_sms, s), "tile samples");
   RTNN_CU(cudaStreamSynchronize(s), "synchronize");
-  std::vector<float> tgt(n_queries);
-  for (uint64_t i = 0; i < n_queries; ++i) {
-    const float d = kth[i] >= 0.f ? std::max(kth[i], 1e-6f * radius) : 1.5f * radius;
-    tgt[i] = std::log(d / cz[i]);
-  }
-  RTNN_CU(cudaMemcpyAsync(d_target, tgt.data(), n_queries * 4, cudaMemcpyHostToDevice, s), "copy");
-  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  *n_samples = sh.n_tiles;
   return RTNN_OK;
 }
 
@@ -1034,10 +1066,10 @@ rtnn_status rtnn_query_widths(rtnn_ctx* c, const float* d_points, uint64_t n_poi
   RTNN_CU(ensure(c->ws.out, (size_t)n_queries * k * 4), "alloc rows");
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
   const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
-  st = run_search(c, sh, pr, d_points, d_queries, (int32_t*)c->ws.out.p, nullptr);
+  // the first search pass writes the width it searched each query at (per query for the
+  // analytic partition, per tile for the learned widths)
+  st = run_search(c, sh, pr, d_points, d_queries, (int32_t*)c->ws.out.p, nullptr, d_widths);
   if (st != RTNN_OK) return st;
-  RTNN_CU(cudaMemcpyAsync(d_widths, c->ws.qwidth_in.p, n_queries * 4, cudaMemcpyDeviceToDevice, s),
-          "copy widths");
   RTNN_CU(cudaStreamSynchronize(s), "synchronize");
   return RTNN_OK;
 }
@@ -1073,6 +1105,81 @@ rtnn_status rtnn_mlp_adam_step(rtnn_ctx* c, float* d_params, const float* d_grad
   RTNN_CU(launch_mlp_adam(d_params, d_grad, d_m, d_v, lr, 0.9f, 0.999f, 1e-8f, step, grad_scale, s),
           "adam");
   RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_layout(rtnn_ctx* c, uint32_t* point_order, uint64_t n_points,
+                        uint32_t* query_order, uint64_t n_queries, uint32_t flags) {
+  if (!c) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  if (!c->layout_valid)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT,
+                "no search to describe: the last rtnn_search / rtnn_search_batched call on this "
+                "context failed, had no points or queries, or ran in host sub-batches (use "
+                "RTNN_FLAG_REF_LAYOUT, which keeps one batch)");
+  if (flags & ~RTNN_FLAG_DEVICE_POINTERS)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "flags: only RTNN_FLAG_DEVICE_POINTERS");
+  if ((point_order && n_points != c->layout_n) || (query_order && n_queries != c->layout_q))
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT,
+                "n_points / n_queries must be those of the last search (" +
+                    std::to_string(c->layout_n) + " / " + std::to_string(c->layout_q) + ")");
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  const cudaMemcpyKind kind = (flags & RTNN_FLAG_DEVICE_POINTERS) ? cudaMemcpyDeviceToDevice
+                                                                  : cudaMemcpyDeviceToHost;
+  // the fourth word of each sorted float4 {x, y, z, caller index}
+  if (point_order && n_points)
+    RTNN_CU(cudaMemcpy2DAsync(point_order, 4, (const char*)c->ws.spts.p + 12, 16, 4, n_points,
+                              kind, s),
+            "copy point order");
+  if (query_order && n_queries)
+    RTNN_CU(cudaMemcpy2DAsync(query_order, 4, (const char*)c->ws.sq.p + 12, 16, 4, n_queries,
+                              kind, s),
+            "copy query order");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  return RTNN_OK;
+}
+
+rtnn_status rtnn_sort_pairs(rtnn_ctx* c, void* d_keys, uint32_t key_bytes, uint32_t* d_values,
+                            uint64_t n, uint32_t key_bits) {
+  if (!c) return RTNN_ERR_INVALID_ARGUMENT;
+  c->err.clear();
+  if (key_bytes != 4 && key_bytes != 8)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "key_bytes must be 4 or 8");
+  if (key_bits == 0 || key_bits > 8 * key_bytes)
+    return fail(c, RTNN_ERR_INVALID_ARGUMENT, "key_bits must be in [1, 8 * key_bytes]");
+  if (n >= (1ull << 31)) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 pairs");
+  if (n == 0) return RTNN_OK;
+  if (!d_keys || !d_values) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "NULL device pointer");
+  cudaSetDevice(c->device);
+  cudaStream_t s = stream_of(c);
+  const bool key64 = key_bytes == 8;
+  const uint64_t rt = radix_tiles_for(n);
+  RTNN_CU(ensure(c->ws.keys1, n * key_bytes), "alloc keys");
+  RTNN_CU(ensure(c->ws.vals1, n * 4), "alloc values");
+  RTNN_CU(ensure(c->ws.hist, 256 * rt * 4), "alloc radix histogram");
+  RTNN_CU(ensure(c->ws.scan_state, scan_tiles_for(256 * rt) * 8), "alloc scan state");
+  RTNN_CU(ensure(c->ws.counters, sizeof(Counters)), "alloc counters");
+  Counters* ctr = (Counters*)c->ws.counters.p;
+  RTNN_CU(cudaMemsetAsync(ctr, 0, sizeof(Counters), s), "memset counters");
+  bool in1 = false;
+  RTNN_CU(radix_sort_pairs(key64, d_keys, d_values, c->ws.keys1.p, (uint32_t*)c->ws.vals1.p,
+                           (uint32_t)n, key_bits, false, (uint32_t*)c->ws.hist.p,
+                           (uint64_t*)c->ws.scan_state.p, &ctr->scan_tiles[0], ctr, &in1, s),
+          "radix sort");
+  if (in1) {   // an odd number of passes: the sorted pairs are in the context's buffers
+    RTNN_CU(cudaMemcpyAsync(d_keys, c->ws.keys1.p, n * key_bytes, cudaMemcpyDeviceToDevice, s),
+            "copy keys");
+    RTNN_CU(cudaMemcpyAsync(d_values, c->ws.vals1.p, n * 4, cudaMemcpyDeviceToDevice, s),
+            "copy values");
+  }
+  RTNN_CU(cudaMemcpyAsync(c->h_ctr, ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "copy");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  if (c->h_ctr->error == kErrScanTimeout)
+    return fail(c, RTNN_ERR_DEVICE_TIMEOUT, "scan look-back gave up waiting on tile " +
+                                                std::to_string(c->h_ctr->error_info));
+  if (c->h_ctr->error != 0)
+    return fail(c, RTNN_ERR_INTERNAL, "device error " + std::to_string(c->h_ctr->error));
   return RTNN_OK;
 }
 

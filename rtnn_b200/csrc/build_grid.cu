@@ -250,12 +250,13 @@ k_count(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Clou
   }
 }
 
-// Scatter into cell-sorted float4 {x, y, z, original index}.
+// Scatter into cell-sorted float4 {x, y, z, original index}. sorted_pos (optional): the
+// inverse map, sorted_pos[original index] = position in spts.
 __global__ void __launch_bounds__(256)
 k_scatter(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, CloudTables t,
           const CloudGrid* __restrict__ grids, const uint32_t* __restrict__ cells,
           const uint32_t* __restrict__ rank, float4* __restrict__ spts, uint32_t n_points,
-          Counters* ctr) {
+          uint32_t* __restrict__ sorted_pos, Counters* ctr) {
   __shared__ float s_xyz[kChunk * 3];
   const ChunkRange r = chunk_range(t.chunk_base, t.point_off, t.n_clouds, blockIdx.x);
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
@@ -269,6 +270,7 @@ k_scatter(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cl
     const uint32_t pos = cells[cell] + rank[r.begin + i];
     if (pos >= n_points) { set_error(ctr, kErrIndexRange, r.begin + i); continue; }
     spts[pos] = make_float4(x, y, z, __uint_as_float(r.begin + i));
+    if (sorted_pos) sorted_pos[r.begin + i] = pos;
   }
 }
 
@@ -370,10 +372,10 @@ cudaError_t launch_count(const float* xyz, uint64_t n_points, bool aligned, cons
 cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
                            const CloudTables& t, uint32_t n_chunks, const CloudGrid* grids,
                            const uint32_t* cells, const uint32_t* rank, float4* spts,
-                           Counters* ctr, cudaStream_t s) {
+                           Counters* ctr, cudaStream_t s, uint32_t* sorted_pos) {
   if (n_chunks == 0) return cudaSuccess;
   k_scatter<<<n_chunks, 256, 0, s>>>(xyz, 3 * n_points, aligned, t, grids, cells, rank, spts,
-                                     (uint32_t)n_points, ctr);
+                                     (uint32_t)n_points, sorted_pos, ctr);
   return cudaGetLastError();
 }
 

@@ -40,6 +40,14 @@ struct SearchArgs {
   uint32_t flags;              // kSearch*
   uint32_t index_base;         // added to every point index written (0 unless the points
                                // passed are a part of the caller's array)
+  const uint32_t* ref_ppos;    // reference layout: row = the query's sorted position, entry =
+                               // ref_ppos[point index] (its position in spts); nullptr: the
+                               // caller's layout (row = query index, entry = point index)
+  const float* model;          // learned widths: MLP parameters; the main pass searches each
+                               // tile (bucket) at its predicted width (tile_model.cuh);
+                               // nullptr: qwidth or the full radius
+  float margin;                // learned width = margin * predicted K-th distance
+  float* width_out;            // optional: the main-pass width of each query (query index)
   int pass;                    // kPassMain, kPassEscalate or kPassFinal
   float lane_walk_ratio;       // tile spread > ratio * width: per-lane walk (0: never)
   float gap_ratio;             // split a tile where consecutive queries are farther apart
@@ -75,10 +83,11 @@ cudaError_t launch_zero_cells(uint32_t* cells, const Counters* ctr, int n_sms, c
 cudaError_t launch_count(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
                          uint32_t n_chunks, const CloudGrid* grids, uint32_t* cells,
                          uint32_t* rank, Counters* ctr, cudaStream_t s);
+// sorted_pos (optional): written with each point's position in spts (the inverse map)
 cudaError_t launch_scatter(const float* xyz, uint64_t n_points, bool aligned,
                            const CloudTables& t, uint32_t n_chunks, const CloudGrid* grids,
                            const uint32_t* cells, const uint32_t* rank, float4* spts,
-                           Counters* ctr, cudaStream_t s);
+                           Counters* ctr, cudaStream_t s, uint32_t* sorted_pos = nullptr);
 cudaError_t launch_query_keys(const float* xyz, uint64_t n_queries, bool aligned,
                               const CloudTables& t, uint32_t n_qchunks, const CloudGrid* grids,
                               uint32_t order_bits, const float* qwidth, float radius,
@@ -93,6 +102,8 @@ constexpr size_t kSearchSmemLimit = 227 * 1024;   // dynamic shared memory per b
 size_t search_smem_bytes(uint32_t k, uint32_t pending, int warps_per_block);
 cudaError_t search_prepare(int device);
 int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block);
+// K itself when the searches have an instantiation with K compiled in, else 0
+int search_compiled_k(uint32_t k);
 // appended-hit slots (multiple of 4, 8..256) and warps per block that fit the limit
 void fit_search_shape(uint32_t k, uint32_t pending_req, int wpb_req, uint32_t* pending, int* wpb);
 // one warp per query (k_search_q): buffer size for k, occupancy and launch
@@ -118,6 +129,7 @@ constexpr int kNormParams = 2 * kFeatDim + 2;
 constexpr int kTrainParams = kHidden * kFeatDim + kHidden + kHidden * kHidden + kHidden + kHidden + 1;
 constexpr int kModelParams = kNormParams + kTrainParams;
 
+// analytic partition (RTNN_FLAG_PARTITION): a width per query from the box counts
 struct WidthArgs {
   CloudTables t;
   const CloudGrid* grids;
@@ -130,13 +142,26 @@ struct WidthArgs {
   float radius;
   uint32_t need;          // points a width must enclose (K + 1)
   float alpha;            // analytic width = alpha * (s* + 1) * cell
-  const float* model;     // learned: MLP parameters (nullptr: analytic)
-  float margin;           // learned width = margin * predicted K-th distance
-  float* qwidth;          // out: per sorted query width (>= radius means full radius)
-  float* feats;           // optional out: [query index][kFeatDim] features (original order)
-  float* cellsz;          // optional out: [query index] cell edge of the query's cloud
+  float* qwidth;          // out: per query width, caller order (>= radius means full radius)
 };
 cudaError_t launch_widths(const WidthArgs& a, int n_sms, cudaStream_t s);
+
+// learned widths: one training sample per tile (bucket) of a plain search -- the tile's
+// features (tile_model.cuh) and target log(largest K-th distance of its queries / cell)
+struct TileSampleArgs {
+  CloudTables t;
+  const CloudGrid* grids;
+  const uint32_t* cells;
+  const uint32_t* total_cells;  // cells in use (device)
+  const float4* sq;             // the search's sorted queries {x, y, z, query index}
+  const float* kth;             // K-th neighbor distance per query index (-1: fewer than K)
+  uint32_t n_tiles;
+  uint32_t need;                // K + 1
+  float radius;
+  float* feats;                 // out: [tile][kFeatDim]
+  float* target;                // out: [tile]
+};
+cudaError_t launch_tile_samples(const TileSampleArgs& a, int n_sms, cudaStream_t s);
 
 // MLP training (hand-written forward / backward / Adam), mlp.cu
 struct MlpBatch {

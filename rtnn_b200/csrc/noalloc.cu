@@ -16,7 +16,10 @@
 // In host code the array's name is only a host-side stand-in: its device address is
 // looked up with cudaGetSymbolAddress once per device (with that device current) on the
 // first call made on that device, which is why that first call should come before any
-// stream capture begins.
+// stream capture begins. The address is cached for the life of the process, so a
+// cudaDeviceReset after the first call on a device is not supported. Beside a global-mode
+// capture on another thread the caller passes a non-blocking stream: the legacy default
+// stream would wait on the capturing stream and break its capture.
 #include <cstring>
 #include <mutex>
 

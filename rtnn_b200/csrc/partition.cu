@@ -1,4 +1,4 @@
-// partition.cu -- density buckets: a search width per query, analytic or learned.
+// partition.cu -- density buckets: search widths, analytic or learned, and the width model.
 //
 // Replaces the reference's query partitioning (src/optixNSearch/):
 //   calcSearchSize / kGenCellMask (grid.cu:84-211, 354-382): per occupied cell, grow a
@@ -7,22 +7,28 @@
 //   sortGenBatch / genBatches / radiusFromMegacell (sort.cpp:262-269, 346-391, 393-498):
 //     queries grouped by that width, each group launched with radius 0.62 * width
 //     (approxMode 2, radiusEquiVolume, util.cpp:422-426).
-// Here every query reads the box counts N_s (s = 0..2 cells around its cell) straight
-// from the scanned cell offsets (one subtraction per row of cells), and gets
-//   analytic: w = alpha * (s* + 1) * cell, s* = first s with N_s >= K + 1
-//             (alpha = 1.24 reproduces the reference's equal-volume radius), or
-//   learned:  w = margin * cell * exp(MLP(features)), the MLP predicting
-//             log(K-th neighbor distance / cell) from the bucket's occupancy histogram
-//             (shell counts) and its extent (cell / r).
+// Analytic (k_widths): every query reads the box counts N_s (s = 0..2 cells around its
+// cell) straight from the scanned cell offsets (one subtraction per row of cells) and gets
+//   w = alpha * (s* + 1) * cell, s* = first s with N_s >= K + 1
+// (alpha = 1.24 reproduces the reference's equal-volume radius); the width's level then
+// joins the query sort key, so a tile shares one width band.
+// Learned: the bucket is the search's 32-query tile, and the search kernel itself predicts
+// its width from the tile's features (tile_model.cuh). This file holds the width model's
+// training: one sample per tile of a plain search (k_tile_samples), and the hand-written
+// loss/gradient, Adam and inference kernels of the MLP.
 // A width >= r means "search at r". Exactness never depends on w: the search kernel
-// re-searches at r every query that finds fewer than K neighbors inside w.
+// re-searches wider every query that finds fewer than K neighbors inside w.
 #include "common.cuh"
 #include "kernels.h"
+#include "tile_model.cuh"
 
 namespace rtnn {
 namespace {
 
 // ---- MLP (6 -> 32 -> 32 -> 1, ReLU) ------------------------------------------------
+static_assert(kFeatDim == kTileFeat && kHidden == kTileHidden,
+              "the trained MLP is the one the search evaluates");
+
 struct MlpView {
   const float* in_mean; const float* in_std; float out_mean, out_std;
   const float* W1; const float* b1; const float* W2; const float* b2; const float* W3; float b3;
@@ -127,12 +133,19 @@ __device__ __forceinline__ void box_counts3(const CloudGrid& g, const uint32_t* 
   N[2] = n2;
 }
 
+__device__ __forceinline__ float wmin_f(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float wmax_f(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 __global__ void __launch_bounds__(256)
 k_widths(WidthArgs a) {
-  __shared__ float s_model[kModelParams];
-  __shared__ __align__(8) float s_w2p[kHidden * kHidden];   // W2, unit pairs interleaved
-  if (a.model) load_model_smem(a.model, s_model, s_w2p);
-  const MlpView mv = mlp_view(s_model);
   const uint32_t total_cells = a.total_cells ? *a.total_cells : 0u;
   // queries that are the points are taken in cell order (neighbouring threads read the
   // same cell rows); only the points placed in cells are there, the rest keep no width
@@ -161,34 +174,55 @@ k_widths(WidthArgs a) {
     const int cz = clamp_cell(cell_coord_f(qz, g.oz, g.inv_cell), g.dz);
     uint32_t N[kShells];
     box_counts3(g, a.cells, cx, cy, cz, N);
-    // offset of the query from its cell's centre, in cells (0 .. 0.87)
-    const float ox = (qx - g.ox) * g.inv_cell - ((float)cx + 0.5f);
-    const float oy = (qy - g.oy) * g.inv_cell - ((float)cy + 0.5f);
-    const float oz = (qz - g.oz) * g.inv_cell - ((float)cz + 0.5f);
-    float feat[kFeatDim];
-    feat[0] = log1pf((float)N[0]);
-    feat[1] = log1pf((float)(N[1] - N[0]));
-    feat[2] = log1pf((float)(N[2] - N[1]));
-    feat[3] = logf((float)a.need) - log1pf((float)N[2]);
-    feat[4] = logf(g.cell / a.radius);
-    feat[5] = fminf(sqrtf(ox * ox + oy * oy + oz * oz), 1.f);
-    float w;
-    if (a.model) {
-      const float o = mlp_forward_norm_x2(mv, s_w2p, feat);
-      const float y = fmaf(o, mv.out_std, mv.out_mean);
-      w = a.margin * g.cell * expf(fminf(y, 30.f));
-    } else {
-      w = INFINITY;
+    float w = INFINITY;
 #pragma unroll
-      for (int s = 0; s < kShells; ++s)
-        if (w == INFINITY && N[s] >= a.need) w = a.alpha * (float)(s + 1) * g.cell;
-    }
+    for (int s = 0; s < kShells; ++s)
+      if (w == INFINITY && N[s] >= a.need) w = a.alpha * (float)(s + 1) * g.cell;
     a.qwidth[i] = (w < a.radius) ? w : a.radius;
-    if (a.feats) {
+  }
+}
+
+// One training sample per tile of a plain search: the tile's features (the same function
+// the search evaluates) and log(largest K-th neighbor distance of its queries / cell);
+// queries with fewer than K neighbors within r do not count (a tile made only of them
+// gets log(1.5 r / cell), beyond the radius). One warp per tile.
+__global__ void __launch_bounds__(256)
+k_tile_samples(TileSampleArgs a) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t total_cells = *a.total_cells;
+  for (uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < a.n_tiles;
+       tile += warps) {
+    uint32_t c = 0;
+    if (lane == 0) c = find_cloud(a.t.tile_base, a.t.n_clouds, tile);
+    const uint32_t cloud = __shfl_sync(0xffffffffu, c, 0);
+    const uint32_t pos = a.t.query_off[cloud] + (tile - a.t.tile_base[cloud]) * 32u + lane;
+    bool valid = pos < a.t.query_off[cloud + 1];
+    const float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
+    valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
+    const float kq = valid ? a.kth[__float_as_uint(q.w)] : -1.f;
+    const float bx0 = wmin_f(valid ? q.x : INFINITY), bx1 = wmax_f(valid ? q.x : -INFINITY);
+    const float by0 = wmin_f(valid ? q.y : INFINITY), by1 = wmax_f(valid ? q.y : -INFINITY);
+    const float bz0 = wmin_f(valid ? q.z : INFINITY), bz1 = wmax_f(valid ? q.z : -INFINITY);
+    const float kmax = wmax_f(kq);
+    const CloudGrid g = a.grids[cloud];
+    const bool ok = __any_sync(0xffffffffu, valid) &&
+                    (uint64_t)g.cell_base + g.n_cells <= (uint64_t)total_cells;
+    float feat[kTileFeat];
+    if (ok) {
+      tile_features(g, a.cells, bx0, bx1, by0, by1, bz0, bz1, a.need, a.radius, feat);
+    } else {
 #pragma unroll
-      for (int f = 0; f < kFeatDim; ++f) a.feats[(size_t)i * kFeatDim + f] = feat[f];
+      for (int f = 0; f < kTileFeat; ++f) feat[f] = 0.f;
     }
-    if (a.cellsz) a.cellsz[i] = g.cell;
+    const float d = kmax >= 0.f ? fmaxf(kmax, 1e-6f * a.radius) : 1.5f * a.radius;
+    if (lane < kTileFeat) {
+      float v = feat[0];
+#pragma unroll
+      for (int f = 1; f < kTileFeat; ++f) v = lane == f ? feat[f] : v;
+      a.feats[(size_t)tile * kTileFeat + lane] = v;
+    }
+    if (lane == 0) a.target[tile] = logf(d / g.cell);
   }
 }
 
@@ -343,6 +377,13 @@ cudaError_t launch_widths(const WidthArgs& a, int n_sms, cudaStream_t s) {
   if (a.n_queries == 0) return cudaSuccess;
   const unsigned blocks = (unsigned)min((uint64_t)n_sms * 8, ((uint64_t)a.n_queries + 255) / 256);
   k_widths<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile_samples(const TileSampleArgs& a, int n_sms, cudaStream_t s) {
+  if (a.n_tiles == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)min((uint64_t)n_sms * 8, ((uint64_t)a.n_tiles + 7) / 8);
+  k_tile_samples<<<blocks, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -20,7 +20,7 @@ constexpr int kSub = 32 * kRadixItems;   // keys per warp sub-tile
 
 template <typename KeyT>
 __global__ void __launch_bounds__(kRadixThreads)
-k_radix_hist(const KeyT* __restrict__ keys, uint32_t n, uint32_t shift,
+k_radix_hist(const KeyT* __restrict__ keys, uint32_t n, uint32_t shift, uint32_t dmask,
              uint32_t* __restrict__ hist, uint32_t n_tiles) {
   __shared__ uint32_t s_h[kWarps][256];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -30,7 +30,7 @@ k_radix_hist(const KeyT* __restrict__ keys, uint32_t n, uint32_t shift,
 #pragma unroll 4
   for (int it = 0; it < kRadixItems; ++it) {
     const uint32_t i = base + it * 32 + lane;
-    if (i < n) atomicAdd(&s_h[warp][(uint32_t)(keys[i] >> shift) & 0xffu], 1u);
+    if (i < n) atomicAdd(&s_h[warp][(uint32_t)(keys[i] >> shift) & dmask], 1u);
   }
   __syncthreads();
   for (int d = threadIdx.x; d < 256; d += blockDim.x) {
@@ -45,7 +45,8 @@ template <typename KeyT>
 __global__ void __launch_bounds__(kRadixThreads)
 k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 KeyT* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
-                uint32_t shift, const uint32_t* __restrict__ offsets, uint32_t n_tiles) {
+                uint32_t shift, uint32_t dmask, const uint32_t* __restrict__ offsets,
+                uint32_t n_tiles) {
   __shared__ uint32_t s_cnt[kWarps][256];   // per warp and digit: count, then tile position
   __shared__ uint32_t s_start[256];         // per digit: first tile position
   __shared__ uint32_t s_dst[256];           // per digit: global offset minus s_start
@@ -66,7 +67,7 @@ k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ v
     const bool valid = i < n;
     k[it] = valid ? keys_in[i] : (KeyT)0;
     v[it] = valid ? (vals_in ? vals_in[i] : i) : 0u;
-    const uint32_t digit = valid ? ((uint32_t)(k[it] >> shift) & 0xffu) : 256u;
+    const uint32_t digit = valid ? ((uint32_t)(k[it] >> shift) & dmask) : 256u;
     const uint32_t peers = __match_any_sync(0xffffffffu, digit);
     uint32_t before = 0;
     if (valid) before = s_cnt[warp][digit];
@@ -111,7 +112,7 @@ k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ v
   for (int it = 0; it < kRadixItems; ++it) {
     const uint32_t i = base + it * 32 + lane;
     if (i < n) {
-      const uint32_t digit = (uint32_t)(k[it] >> shift) & 0xffu;
+      const uint32_t digit = (uint32_t)(k[it] >> shift) & dmask;
       const uint32_t li = s_cnt[warp][digit] + rk[it];
       s_keys[li] = k[it];
       s_vals[li] = v[it];
@@ -122,7 +123,7 @@ k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ v
   const uint32_t count = min((uint32_t)kRadixTile, n - blockIdx.x * (uint32_t)kRadixTile);
   for (uint32_t j = threadIdx.x; j < count; j += blockDim.x) {
     const KeyT key = s_keys[j];
-    const uint32_t dst = s_dst[(uint32_t)(key >> shift) & 0xffu] + j;
+    const uint32_t dst = s_dst[(uint32_t)(key >> shift) & dmask] + j;
     keys_out[dst] = key;
     vals_out[dst] = s_vals[j];
   }
@@ -132,7 +133,7 @@ k_radix_scatter(const KeyT* __restrict__ keys_in, const uint32_t* __restrict__ v
 
 uint32_t radix_tiles_for(uint64_t n) { return (uint32_t)((n + kRadixTile - 1) / kRadixTile); }
 
-// Sorts n pairs on bits [0, bits). Ping-pongs between (keys0, vals0) and (keys1, vals1);
+// Sorts n pairs on bits [0, bits) (bits above are ignored). Ping-pongs between (keys0, vals0) and (keys1, vals1);
 // *result_in_1 tells where the sorted pairs ended up. identity_values: the first pass
 // reads value i for position i instead of vals0.
 cudaError_t radix_sort_pairs(bool key64, void* keys0, uint32_t* vals0, void* keys1,
@@ -151,22 +152,24 @@ cudaError_t radix_sort_pairs(bool key64, void* keys0, uint32_t* vals0, void* key
     const uint32_t* vin = (p == 0 && identity_values) ? nullptr : (in1 ? vals1 : vals0);
     uint32_t* vout = in1 ? vals0 : vals1;
     const uint32_t shift = 8 * p;
+    // the last pass sorts only the bits below `bits` (keys may hold more above them)
+    const uint32_t dmask = bits - shift >= 8 ? 0xffu : (1u << (bits - shift)) - 1u;
     if (key64)
-      k_radix_hist<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint64_t*)kin, n, shift, hist,
-                                                                n_tiles);
+      k_radix_hist<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint64_t*)kin, n, shift,
+                                                                dmask, hist, n_tiles);
     else
-      k_radix_hist<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint32_t*)kin, n, shift, hist,
-                                                                n_tiles);
+      k_radix_hist<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>((const uint32_t*)kin, n, shift,
+                                                                dmask, hist, n_tiles);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const uint64_t hn = 256ull * n_tiles;
     e = launch_scan_excl(hist, hn, nullptr, 0, hn, scan_state, scan_counters + p, ctr, s);
     if (e != cudaSuccess) return e;
     if (key64)
       k_radix_scatter<uint64_t><<<n_tiles, kRadixThreads, 0, s>>>(
-          (const uint64_t*)kin, vin, (uint64_t*)kout, vout, n, shift, hist, n_tiles);
+          (const uint64_t*)kin, vin, (uint64_t*)kout, vout, n, shift, dmask, hist, n_tiles);
     else
       k_radix_scatter<uint32_t><<<n_tiles, kRadixThreads, 0, s>>>(
-          (const uint32_t*)kin, vin, (uint32_t*)kout, vout, n, shift, hist, n_tiles);
+          (const uint32_t*)kin, vin, (uint32_t*)kout, vout, n, shift, dmask, hist, n_tiles);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     in1 = !in1;
   }

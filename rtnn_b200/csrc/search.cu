@@ -28,6 +28,7 @@
 // and the last pass at the full radius, so every row is exact.
 #include "common.cuh"
 #include "kernels.h"
+#include "tile_model.cuh"
 
 namespace rtnn {
 namespace {
@@ -46,6 +47,46 @@ __device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t i, uint32_t
     i = c;
   }
   h[i * 32] = x;
+}
+
+// Depth of a K-entry heap below its root: floor(log2(K)).
+__host__ __device__ constexpr int heap_depth(int k) { return k <= 1 ? 0 : 1 + heap_depth(k / 2); }
+
+// heap_sift_down for a compile-time K, starting at node I: a fixed number of levels, every
+// step predicated instead of branched, so that the 32 lanes of a warp (each sifting its
+// own heap) stay on one path. A level whose nodes all have two children skips the bound
+// checks (decided at compile time, the level being a constant of the unrolled loop).
+template <int K, int I>
+__device__ __forceinline__ void heap_sift_fixed(uint64_t* h, uint64_t x) {
+  constexpr int kLevels = heap_depth(K) - heap_depth(I + 1);
+  uint32_t i = I;
+  bool go = true;
+#pragma unroll
+  for (int l = 0; l < kLevels; ++l) {
+    // nodes of this level: [(I + 1) * 2^l - 1, (I + 2) * 2^l - 2]
+    const int last = (I + 2) * (1 << l) - 2;
+    const bool all_two = 2 * last + 2 < K;   // constant per unrolled level
+    const uint32_t c = 2 * i + 1;
+    const bool has1 = all_two || c < (uint32_t)K;
+    const bool has2 = all_two || c + 1 < (uint32_t)K;
+    uint64_t cv = has1 ? h[c * 32] : 0ull;
+    const uint64_t c2 = has2 ? h[(c + 1) * 32] : 0ull;
+    const bool right = c2 > cv;
+    cv = right ? c2 : cv;
+    const bool move = go && has1 && cv > x;
+    if (move) h[i * 32] = cv;
+    go = move;
+    i = move ? c + (right ? 1u : 0u) : i;
+  }
+  h[i * 32] = x;
+}
+
+template <int K, int I = K / 2 - 1>
+__device__ __forceinline__ void heapify_fixed(uint64_t* h) {
+  if constexpr (I >= 0) {
+    heap_sift_fixed<K, I>(h, h[I * 32]);
+    heapify_fixed<K, I - 1>(h);
+  }
 }
 
 // ---- packed FP32x2 arithmetic (sm_100a): two IEEE round-to-nearest operations per
@@ -100,6 +141,7 @@ __device__ __forceinline__ float4 stage_get(const float* st, uint32_t slot) {
 }
 
 constexpr int kCheck = 4;          // candidates tested between two buffer-full votes
+constexpr uint32_t kFixedPending = 16;   // appended-hit slots of the compiled-K searches
 constexpr uint32_t kQueryCap = 128;   // k_search_q hit buffer per warp (k <= 64)
 constexpr int kStage = 64;         // staged candidates per warp (float4)
 constexpr uint64_t kRowStride = 4294967311ull;   // prime > 2^32 > any row count of a box
@@ -224,14 +266,22 @@ struct LaneTop {
 // Folds slots [n, fill) into the kept set. With any_k the first k hits are kept as they
 // came and later ones dropped. Out of line: it is reached from several places of the
 // test loop, and one copy keeps the hot loop small enough for the instruction cache.
+// KC > 0: k == KC is a compile-time constant and the heap steps are the branch-free
+// fixed-depth ones (heap_sift_fixed); KC == 0: any k, data-dependent loops.
+template <int KC>
 __device__ __noinline__ LaneTop merge_column(uint64_t* col, LaneTop s, uint32_t k, bool any_k) {
+  if constexpr (KC > 0) k = KC;
   if (s.n < k) {
     if (s.fill < k || any_k) {   // at exactly k the heap is built below
       s.n = min(s.fill, k);
       s.fill = s.n;
       return s;
     }
-    for (int i = (int)k / 2 - 1; i >= 0; --i) heap_sift_down(col, (uint32_t)i, k, col[i * 32]);
+    if constexpr (KC > 0) {
+      heapify_fixed<KC>(col);
+    } else {
+      for (int i = (int)k / 2 - 1; i >= 0; --i) heap_sift_down(col, (uint32_t)i, k, col[i * 32]);
+    }
     s.root = col[0];
     s.n = k;
   }
@@ -245,7 +295,8 @@ __device__ __noinline__ LaneTop merge_column(uint64_t* col, LaneTop s, uint32_t 
   for (uint32_t j = k; j < s.fill; ++j) {
     const uint64_t next = j + 1 < s.fill ? col[(j + 1) * 32] : 0ull;
     if (key < root) {
-      heap_sift_down(col, 0, k, key);
+      if constexpr (KC > 0) heap_sift_fixed<KC, 0>(col, key);
+      else heap_sift_down(col, 0, k, key);
       root = col[0];
     }
     key = next;
@@ -270,18 +321,38 @@ __device__ __forceinline__ float wmax(float v) {
   return v;
 }
 
-template <bool KNN>
+// Learned widths, main pass: the width of the tile (the bucket; every lane the same value)
+// from its features -- the bounding box of its searchable queries and the box counts
+// around its centre -- through the width model (tile_model.cuh). A tile with no searchable
+// query, or a grid that overran the cell array, keeps the full radius.
+__device__ __forceinline__ float learned_tile_width(const SearchArgs& a, uint32_t cloud,
+                                                   const float4& q, bool valid,
+                                                   uint32_t total_cells) {
+  if (!__any_sync(0xffffffffu, valid)) return a.radius;
+  const float bx0 = wmin(valid ? q.x : INFINITY), bx1 = wmax(valid ? q.x : -INFINITY);
+  const float by0 = wmin(valid ? q.y : INFINITY), by1 = wmax(valid ? q.y : -INFINITY);
+  const float bz0 = wmin(valid ? q.z : INFINITY), bz1 = wmax(valid ? q.z : -INFINITY);
+  const CloudGrid g = a.grids[cloud];
+  if ((uint64_t)g.cell_base + g.n_cells > (uint64_t)total_cells) return a.radius;
+  return tile_width(g, a.cells, a.model, a.margin, bx0, bx1, by0, by1, bz0, bz1, a.k + 1,
+                    a.radius);
+}
+
+// KC > 0: the search for K == KC compiled in (the reference compiles its K in,
+// camera.cu:66-72, CMakeLists.txt:58-61), with kFixedPending appended-hit slots, so the
+// column length and every heap loop bound are constants; KC == 0: any K and slot count.
+template <bool KNN, int KC>
 __global__ void __launch_bounds__(256, 2)
 k_search(SearchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   float* stage = reinterpret_cast<float*>(smem) + warp * kStage * 4;   // pair layout
-  const uint32_t slots = a.k + a.pending;   // result column length per lane
+  const uint32_t k = KC > 0 ? (uint32_t)KC : a.k;
+  const uint32_t slots = k + (KC > 0 ? kFixedPending : a.pending);   // column length per lane
   uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * kStage * 16) +
                     (size_t)warp * slots * 32;
   uint64_t* col = heapw + lane;   // this lane's column: col[i * 32]
   const uint32_t lt = lanemask_lt();
-  const uint32_t k = a.k;
   const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
   const bool local_idx = (a.flags & kSearchLocalIndices) != 0;
   const bool any_k = (a.flags & kSearchAnyK) != 0;
@@ -317,9 +388,11 @@ k_search(SearchArgs a) {
     }
     const bool in_range = valid;
     float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
+    valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
+    if (main_pass && a.model) wq = learned_tile_width(a, cloud, q, valid, total_cells);
+    if (a.width_out && main_pass && in_range) a.width_out[__float_as_uint(q.w)] = wq;
     float w = a.radius, lim = a.r2;
     if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
-    valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
 
     bool short_lane = false;   // narrowed search that found fewer than K neighbors
     // The tile is searched as runs of consecutive queries: a run ends where the next query
@@ -419,7 +492,7 @@ k_search(SearchArgs a) {
       auto check = [&]() {
         if (__any_sync(0xffffffffu, fill > slots - kCheck)) {
           top.fill = fill;
-          top = merge_column(col, top, k, any_k);
+          top = merge_column<KC>(col, top, k, any_k);
           fill = top.fill;
           hit_window(act && !(any_k && top.n >= k), lim_l, root_dist(top, k), KNN, wlo, wspan);
         }
@@ -567,7 +640,7 @@ k_search(SearchArgs a) {
       }
 
       top.fill = fill;
-      top = merge_column(col, top, k, any_k);
+      top = merge_column<KC>(col, top, k, any_k);
       const uint32_t n = top.n;
       if (lane == 0 && loaded) {
         atomicAdd(&a.ctr->n_loaded, (unsigned long long)loaded);
@@ -602,10 +675,14 @@ k_search(SearchArgs a) {
         wm &= wm - 1;
         const uint32_t nL = __shfl_sync(0xffffffffu, n, L);
         const uint32_t qi = __float_as_uint(__shfl_sync(0xffffffffu, q.w, L));
-        int32_t* row = a.out + (size_t)qi * k;
+        const uint32_t pL = __shfl_sync(0xffffffffu, pos, L);
+        int32_t* row = a.out + (size_t)(a.ref_ppos ? pL : qi) * k;
         for (uint32_t jj = lane; jj < k; jj += 32) {
           int32_t v = -1;
-          if (jj < nL) v = (int32_t)((uint32_t)heapw[jj * 32 + L] - sub);
+          if (jj < nL) {
+            const uint32_t pi = (uint32_t)heapw[jj * 32 + L];
+            v = (int32_t)((a.ref_ppos ? __ldg(a.ref_ppos + pi) : pi) - sub);
+          }
           row[jj] = v;
         }
       }
@@ -615,7 +692,9 @@ k_search(SearchArgs a) {
     for (uint32_t m = __ballot_sync(0xffffffffu, in_range && !valid); m; m &= m - 1) {
       const int L = __ffs(m) - 1;
       const uint32_t qi = __float_as_uint(__shfl_sync(0xffffffffu, q.w, L));
-      for (uint32_t jj = lane; jj < k; jj += 32) a.out[(size_t)qi * k + jj] = -1;
+      const uint32_t pL = __shfl_sync(0xffffffffu, pos, L);
+      const size_t ri = a.ref_ppos ? pL : qi;
+      for (uint32_t jj = lane; jj < k; jj += 32) a.out[ri * k + jj] = -1;
     }
     // flag per entry; the compaction keeps the flagged ones in this pass's order
     if (a.fb_flag && in_range) {
@@ -701,7 +780,8 @@ __device__ __noinline__ uint64_t warp_select(uint64_t* buf, uint32_t n, uint32_t
   return warp_sort_keep<4>(buf, n, keep);
 }
 
-template <bool KNN>
+// KC > 0: K == KC compiled in (as for k_search).
+template <bool KNN, int KC>
 // three blocks per SM (80 registers): the walk is latency-bound, more resident warps
 // outweigh the few spills around the out-of-line sort (measured)
 __global__ void __launch_bounds__(256, 3)
@@ -711,7 +791,7 @@ k_search_q(SearchArgs a) {
   const uint32_t cap = a.qcap;   // hit buffer entries per warp: k + 64 <= cap = 128
   uint64_t* buf = reinterpret_cast<uint64_t*>(smem) + (size_t)warp * cap;
   const uint32_t lt = lanemask_lt();
-  const uint32_t k = a.k;
+  const uint32_t k = KC > 0 ? (uint32_t)KC : a.k;
   const bool sorted_rows = (a.flags & kSearchSortedRows) != 0;
   const bool local_idx = (a.flags & kSearchLocalIndices) != 0;
   const bool any_k = (a.flags & kSearchAnyK) != 0;
@@ -748,9 +828,11 @@ k_search_q(SearchArgs a) {
     }
     const bool in_range = valid;
     const float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
+    valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
+    if (main_pass && a.model) wq = learned_tile_width(a, cloud, q, valid, total_cells);
+    if (a.width_out && main_pass && in_range) a.width_out[__float_as_uint(q.w)] = wq;
     float w = a.radius, lim = a.r2;
     if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
-    valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
     bool short_lane = false;
 
     for (uint32_t todo = __ballot_sync(0xffffffffu, in_range); todo; todo &= todo - 1) {
@@ -761,8 +843,9 @@ k_search_q(SearchArgs a) {
       const float wj = __shfl_sync(0xffffffffu, w, j), limj = __shfl_sync(0xffffffffu, lim, j);
       const uint32_t cj = __shfl_sync(0xffffffffu, cloud, j);
       const uint32_t ej = __shfl_sync(0xffffffffu, entry, j);
+      const uint32_t pj = __shfl_sync(0xffffffffu, pos, j);
       const bool vj = __shfl_sync(0xffffffffu, valid ? 1u : 0u, j) != 0u;
-      int32_t* row = a.out + (size_t)qi * k;
+      int32_t* row = a.out + (size_t)(a.ref_ppos ? pj : qi) * k;
       if (!vj) {   // a non-finite coordinate: nothing to search, an empty row
         for (uint32_t jj = lane; jj < k; jj += 32) row[jj] = -1;
         continue;
@@ -876,8 +959,14 @@ k_search_q(SearchArgs a) {
       }
       __syncwarp();
       const uint32_t sub = local_idx ? a.t.point_off[cj] : 0u - a.index_base;
-      for (uint32_t jj = lane; jj < k; jj += 32)
-        row[jj] = jj < found ? (int32_t)((uint32_t)buf[jj] - sub) : -1;
+      for (uint32_t jj = lane; jj < k; jj += 32) {
+        int32_t v = -1;
+        if (jj < found) {
+          const uint32_t pi = (uint32_t)buf[jj];
+          v = (int32_t)((a.ref_ppos ? __ldg(a.ref_ppos + pi) : pi) - sub);
+        }
+        row[jj] = v;
+      }
       __syncwarp();
     }
     if (a.fb_flag && in_range) a.fb_flag[entry] = short_lane ? 1u : 0u;
@@ -933,13 +1022,49 @@ void fit_search_shape(uint32_t k, uint32_t pending_req, int wpb_req, uint32_t* p
   *wpb = w;
 }
 
+// The K values compiled in (a fixed set, as the reference compiles one K per build); any
+// other K, or a k_search slot count other than kFixedPending, runs the generic kernels.
+#define RTNN_COMPILED_KS(X) X(5) X(8) X(16) X(32) X(50) X(64)
+
+namespace {
+int compiled_k(uint32_t k) {
+#define RTNN_CASE(K) if (k == K) return K;
+  RTNN_COMPILED_KS(RTNN_CASE)
+#undef RTNN_CASE
+  return 0;
+}
+
+// kernel entry of k_search / k_search_q for (mode, compiled K or 0)
+const void* search_fn(bool knn, int kc) {
+#define RTNN_CASE(K) if (kc == K) return knn ? (const void*)k_search<true, K> : (const void*)k_search<false, K>;
+  RTNN_COMPILED_KS(RTNN_CASE)
+#undef RTNN_CASE
+  return knn ? (const void*)k_search<true, 0> : (const void*)k_search<false, 0>;
+}
+const void* search_q_fn(bool knn, int kc) {
+#define RTNN_CASE(K) if (kc == K) return knn ? (const void*)k_search_q<true, K> : (const void*)k_search_q<false, K>;
+  RTNN_COMPILED_KS(RTNN_CASE)
+#undef RTNN_CASE
+  return knn ? (const void*)k_search_q<true, 0> : (const void*)k_search_q<false, 0>;
+}
+int tile_kc(uint32_t k, uint32_t pending) { return pending == kFixedPending ? compiled_k(k) : 0; }
+}  // namespace
+
+int search_compiled_k(uint32_t k) { return compiled_k(k); }
+
 cudaError_t search_prepare(int device) {
   (void)device;
-  cudaError_t e = cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kSearchSmemLimit);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaSuccess;
+  for (int knn = 0; knn < 2 && e == cudaSuccess; ++knn) {
+    e = cudaFuncSetAttribute(search_fn(knn, 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kSearchSmemLimit);
+#define RTNN_CASE(K)                                                                           \
+    if (e == cudaSuccess)                                                                      \
+      e = cudaFuncSetAttribute(search_fn(knn, K), cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                               (int)kSearchSmemLimit);
+    RTNN_COMPILED_KS(RTNN_CASE)
+#undef RTNN_CASE
+  }
   return e;
 }
 
@@ -947,8 +1072,8 @@ int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_b
   int nb = 0;
   const size_t smem = search_smem_bytes(k, pending, warps_per_block);
   const int threads = warps_per_block * 32;
-  cudaError_t e = knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<true>, threads, smem)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<false>, threads, smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &nb, search_fn(knn, tile_kc(k, pending)), threads, smem);
   if (e != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }
@@ -963,9 +1088,8 @@ int search_q_blocks_per_sm(bool knn, uint32_t k, int warps_per_block) {
   int nb = 0;
   const size_t smem = search_q_smem_bytes(search_q_cap(k), warps_per_block);
   const int threads = warps_per_block * 32;
-  cudaError_t e =
-      knn ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<true>, threads, smem)
-          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search_q<false>, threads, smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &nb, search_q_fn(knn, compiled_k(k)), threads, smem);
   if (e != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }
@@ -973,17 +1097,19 @@ int search_q_blocks_per_sm(bool knn, uint32_t k, int warps_per_block) {
 cudaError_t launch_search_q(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
                             cudaStream_t s) {
   const size_t smem = search_q_smem_bytes(a.qcap, warps_per_block);
-  if (knn) k_search_q<true><<<blocks, warps_per_block * 32, smem, s>>>(a);
-  else k_search_q<false><<<blocks, warps_per_block * 32, smem, s>>>(a);
-  return cudaGetLastError();
+  SearchArgs args = a;
+  void* params[] = {&args};
+  return cudaLaunchKernel(search_q_fn(knn, compiled_k(a.k)), dim3(blocks),
+                          dim3(warps_per_block * 32), params, smem, s);
 }
 
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
                           cudaStream_t s) {
   const size_t smem = search_smem_bytes(a.k, a.pending, warps_per_block);
-  if (knn) k_search<true><<<blocks, warps_per_block * 32, smem, s>>>(a);
-  else k_search<false><<<blocks, warps_per_block * 32, smem, s>>>(a);
-  return cudaGetLastError();
+  SearchArgs args = a;
+  void* params[] = {&args};
+  return cudaLaunchKernel(search_fn(knn, tile_kc(a.k, a.pending)), dim3(blocks),
+                          dim3(warps_per_block * 32), params, smem, s);
 }
 
 }  // namespace rtnn

@@ -140,3 +140,54 @@ def sph_step(points, h=1.0, sigma=0.05, seed=0):
     """One time step of the SPH configuration: positions perturbed by N(0, sigma*h)."""
     rng = _rng(seed)
     return (points + rng.standard_normal(points.shape) * (sigma * h)).astype(np.float32)
+
+
+def training_clouds(name, scale=1.0, rank=0, count=None):
+    """Clouds of other seeds (never a measured one) whose exact K-th neighbor distances
+    train the width model of workload `name`: [(points, queries or None)], at most
+    `count` of them when given."""
+    s = 1000 * rank + 100
+    out = []
+    if name == "knn_multicloud_4096":
+        p, off = multicloud(n_clouds=96 if count is None else count, seed=s + 7)
+        for c in range(len(off) - 1):
+            out.append((p[int(off[c]):int(off[c + 1])], None))
+    elif name == "knn_surface_1e7":
+        for i in range(20 if count is None else count):
+            out.append((surfaces(seed=s + i, scale=0.05 * max(scale, 0.02)), None))
+    elif name == "knn_gmm_1e6":
+        for i in range(4 if count is None else count):
+            out.append(gmm(seed=s + i, scale=0.25 * scale))
+    elif name == "radius_uniform_1e5":
+        for i in range(4 if count is None else count):
+            out.append((uniform_cube(seed=s + i, scale=scale), None))
+    elif name == "sph_lattice_5e7":
+        for i in range(2 if count is None else count):
+            out.append((sph_lattice(seed=s + i, scale=0.02 * scale), None))
+    else:
+        raise ValueError(f"unknown workload {name}")
+    return out
+
+
+def train_width_model(ctx, name, scale=1.0, rank=0, epochs=32, count=None):
+    """Trains the context's width model for workload `name` on the GPU: exact K-th
+    distances from the plain search over training_clouds(), then the library's own
+    forward/backward/Adam kernels. Returns sample count and first/last epoch loss."""
+    import torch
+    cfg = CONFIGS[name]
+    feats, tgts = [], []
+    for p, q in training_clouds(name, scale, rank, count):
+        tp = torch.from_numpy(np.ascontiguousarray(p)).cuda()
+        tq = None if q is None else torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        f, t = ctx.collect_training(tp, tq, cfg["mode"], cfg["radius"], cfg["k"])
+        feats.append(f)
+        tgts.append(t)
+    f = torch.cat(feats)
+    t = torch.cat(tgts)
+    gen = torch.Generator(device=f.device).manual_seed(0)
+    perm = torch.randperm(f.shape[0], device=f.device, generator=gen)
+    f = f[perm].contiguous()
+    t = t[perm].contiguous()
+    losses = ctx.train_model(f, t, epochs=epochs, batch=16384, lr=3e-3, seed=rank)
+    return {"samples": int(f.shape[0]), "loss_first": float(losses[0]),
+            "loss_last": float(losses[-1])}

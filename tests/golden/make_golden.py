@@ -22,7 +22,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 
-REF_SAMPLE = "/root/reference/src/samplepc.txt"
+# the reference checkout: RTNN_REFERENCE_DIR, the same variable oracle/Makefile reads
+REF_DIR = os.environ.get("RTNN_REFERENCE_DIR", "/root/reference")
+REF_SAMPLE = os.path.join(REF_DIR, "src", "samplepc.txt")
 
 
 def read_reference_csv(path):

@@ -42,6 +42,8 @@ def test_version_and_k_range():
     assert b"sm_100a" in lib.rtnn_version()
     assert lib.rtnn_k_supported(1) == 1 and lib.rtnn_k_supported(rtnn_b200.MAX_K) == 1
     assert lib.rtnn_k_supported(0) == 0 and lib.rtnn_k_supported(rtnn_b200.MAX_K + 1) == 0
+    # the K values with kernels compiled in (the benchmark configurations' K among them)
+    assert [k for k in range(0, 130) if lib.rtnn_k_compiled(k)] == [5, 8, 16, 32, 50, 64]
 
 
 def test_model_size_matches_layout():

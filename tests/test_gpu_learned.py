@@ -153,17 +153,22 @@ def test_learned_widths_are_tighter_than_analytic(ctx):
     assert fb_rate < 0.25
 
 
-def test_width_features_match_oracle_box_counts(ctx):
-    """The shell-count features of the width model (N_0..N_2 box counts around a query's
-    cell) equal the oracle's counts on the same grid (cell and origin from the search)."""
+def test_tile_features_and_targets_match_the_oracle(ctx):
+    """One training sample per 32-query tile of the plain search: the shell-count features
+    (N_0..N_2 box counts around the cell of the tile box's centre) equal the oracle's counts
+    on the same grid (cell and origin from the search), the extent and cell features follow
+    the tile's box, and the target is log(largest K-th neighbor distance / cell) from the
+    oracle's rows."""
     import torch
-    p = wl.uniform_cube(20000, 30.0, seed=12)
+    n, k, r = 20000, 16, 2.0
+    p = wl.uniform_cube(n, 30.0, seed=12)
     tp = torch.from_numpy(p).cuda()
     st = rtnn_b200.Stats()
-    ctx.search(tp, None, "knn", 2.0, 16, partition=True, stats=st)
-    f, _ = ctx.collect_training(tp, None, "knn", 2.0, 16)
-    f = f.cpu().numpy()
-    assert f.shape == (p.shape[0], rtnn_b200.MODEL_FEATURES)
+    ctx.search(tp, None, "knn", r, k, stats=st)
+    f, t = ctx.collect_training(tp, None, "knn", r, k)
+    _, qo = ctx.layout(n, n)   # the sorted order of that plain search: tile t = rows 32t..
+    f, t = f.cpu().numpy(), t.cpu().numpy()
+    assert f.shape == ((n + 31) // 32, rtnn_b200.MODEL_FEATURES) and t.shape == (f.shape[0],)
     cell = np.float32(st.cell_size)
     dims = np.array(list(st.grid_dims))
     o = p.min(0).astype(np.float32)
@@ -171,8 +176,52 @@ def test_width_features_match_oracle_box_counts(ctx):
     ci = np.clip(np.floor((p - o) * inv), 0, dims - 1).astype(np.int64)
     counts = np.zeros(dims[::-1], dtype=np.uint32)
     np.add.at(counts, (ci[:, 2], ci[:, 1], ci[:, 0]), 1)
-    for i in range(0, p.shape[0], 37):
-        N = oracle.box_counts(counts, *ci[i], shells=3).astype(np.float64)
+    rows = oracle.grid_search(p, None, "knn", r, k)
+    for tile in range(0, f.shape[0], 23):
+        q = p[qo[32 * tile:32 * tile + 32].astype(np.int64)]
+        lo, hi = q.min(0), q.max(0)
+        centre = (np.float32(0.5) * (lo + hi)).astype(np.float32)
+        c = np.clip(np.floor((centre - o) * inv), 0, dims - 1).astype(np.int64)
+        N = oracle.box_counts(counts, *c, shells=3).astype(np.float64)
         exp = np.log1p([N[0], N[1] - N[0], N[2] - N[1]])
-        assert np.allclose(f[i, [0, 1, 2]], exp, atol=1e-5), (i, f[i], N)
-        assert abs(f[i, 3] - (np.log(17.0) - np.log1p(N[2]))) <= 1e-5
+        assert np.allclose(f[tile, [0, 1, 2]], exp, atol=1e-5), (tile, f[tile], N)
+        assert abs(f[tile, 3] - (np.log(k + 1.0) - np.log1p(N[2]))) <= 1e-5
+        assert abs(f[tile, 4] - np.log(float(cell) / r)) <= 1e-5
+        ext = float((hi - lo).max()) * float(inv)
+        assert abs(f[tile, 5] - np.log1p(ext)) <= 1e-4
+        qi = qo[32 * tile:32 * tile + 32].astype(np.int64)
+        last = rows[qi, k - 1]
+        have = last >= 0
+        if have.any():
+            d = np.sqrt(((p[qi[have]] - p[last[have]]) ** 2).sum(1)).max()
+            assert abs(t[tile] - np.log(d / float(cell))) <= 1e-4, (tile, t[tile])
+        else:
+            assert abs(t[tile] - np.log(1.5 * r / float(cell))) <= 1e-5
+
+
+def test_learned_tile_widths_cover_most_queries(ctx):
+    """The widths the learned search uses are one per tile (bucket): every query of a tile
+    gets the same width, below r where the data is dense, and the share of queries that
+    need the wider fallback stays small."""
+    import torch
+    _train(ctx)
+    p = torch.from_numpy(_cloud(4)).cuda()
+    w = ctx.query_widths(p, None, "knn", 2.0, 16, learned=True).cpu().numpy()
+    _, qo = ctx.layout(p.shape[0], p.shape[0])
+    ws = w[qo.astype(np.int64)]
+    tiles = ws[: (ws.size // 32) * 32].reshape(-1, 32)
+    assert (tiles == tiles[:, :1]).all()
+    assert np.median(ws) < 2.0
+    # the search's warp-wide MLP gives the width the inference kernel predicts from the
+    # same tile's features (the plain search forms the same tiles)
+    f, _ = ctx.collect_training(p, None, "knn", 2.0, 16)
+    st0 = rtnn_b200.Stats()
+    ctx.search(p, None, "knn", 2.0, 16, stats=st0)
+    y = ctx.mlp_forward(torch.from_numpy(ctx.get_model()).cuda(), f.contiguous()).cpu().numpy()
+    margin = ctx.tuning().width_margin
+    exp_w = np.minimum(margin * st0.cell_size * np.exp(np.minimum(y, 30.0)), 2.0)
+    got_w = ws[0::32][: exp_w.size]
+    assert np.allclose(got_w, exp_w[: got_w.size], rtol=1e-4, atol=1e-6)
+    st = rtnn_b200.Stats()
+    ctx.search(p, None, "knn", 2.0, 16, learned=True, stats=st)
+    assert st.n_fallback < 0.25 * p.shape[0]

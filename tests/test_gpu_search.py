@@ -119,6 +119,28 @@ def test_k_range(ctx, k):
         assert_rows_equal(got, exp, True)
 
 
+@pytest.mark.parametrize("k", [5, 7, 8, 16, 32, 50, 64])
+def test_compiled_k_matches_the_generic_kernels(ctx, k):
+    """K in the compiled set runs kernels with K built in (and 16 appended-hit slots);
+    another slot count, or a K outside the set (7), runs the generic kernels. Both give the
+    oracle's rows, for the tile walk and the one-warp-per-query walk, with many heap
+    replacements (about 48 points within r per query)."""
+    p = wl.uniform_cube(20_000, 30.0, seed=k)
+    base = ctx.tuning().as_dict()
+    try:
+        for mode in ("radius", "knn"):
+            exp = oracle.grid_search(p, None, mode, 2.5, k)
+            for qw in (0, 1):
+                for slots in (16, 20):
+                    ctx.set_tuning(**{**base, "pending_slots": slots, "query_warps": qw})
+                    got = ctx.search(p, None, mode, 2.5, k, sorted_rows=True)
+                    assert_rows_equal(got, exp, True)
+                    got = ctx.search(p, None, mode, 2.5, k)
+                    assert_rows_equal(got, exp, False)
+    finally:
+        ctx.set_tuning(**base)
+
+
 def test_lattice_ties_break_by_index(ctx):
     g = np.stack(np.meshgrid(np.arange(12), np.arange(12), np.arange(12), indexing="ij"), -1)
     p = g.reshape(-1, 3).astype(np.float32)
