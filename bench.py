@@ -90,6 +90,11 @@ def parse():
                          "training step of the width model (loss/gradient, Adam, inference) "
                          "between cudaProfilerStart/Stop, for ncu --profile-from-start off; no "
                          "JSON line")
+    ap.add_argument("--model-file", default=None,
+                    help="--profile: load the width model from this file when it exists, else "
+                         "train it and save it there (the same model across profiled builds)")
+    ap.add_argument("--width-model", type=int, default=0, choices=[0, 1],
+                    help="--profile: the learned widths per query (0) or per tile (1)")
     ap.add_argument("--profile-path", default="learned", choices=["learned", "partition", "plain"],
                     help="--profile: the step profiled (learned widths, the analytic partition "
                          "or the plain grid)")
@@ -109,10 +114,15 @@ def run_profile(args):
     # the first pass and one warp per query for the escalation passes
     ctx.set_tuning(points_per_cell=0.125, cell_ratio=0.125, min_cell_ratio=0.01, width_margin=1.1,
                    fallback_passes=2, gap_ratio=2.0, pending_slots=16, query_warps=2,
-                   buckets_per_halving=1.0)
+                   buckets_per_halving=1.0, width_model=args.width_model)
     learned = args.profile_path == "learned"
     if learned:
-        train_model(ctx, cfg, args.scale, 0)
+        if args.model_file and os.path.exists(args.model_file):
+            ctx.set_model(np.fromfile(args.model_file, dtype=np.float32))
+        else:
+            train_model(ctx, cfg, args.scale, 0)
+            if args.model_file:
+                ctx.get_model().tofile(args.model_file)
         p0, q0 = training_clouds(cfg["name"], args.scale, 0)[0]
         tp0 = torch.from_numpy(np.ascontiguousarray(p0)).cuda()
         tq0 = None if q0 is None else torch.from_numpy(np.ascontiguousarray(q0)).cuda()
@@ -372,7 +382,7 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        return reduce_max(x, dist, "cuda")
+        return reduce_max(x, dist, "cuda" if dist is None or dist.get_backend() == "nccl" else "cpu")
 
     # SPH workload: every step first moves each particle by N(0, 0.05 h), then rebuilds the
     # grid and searches (the rebuild is part of every step anyway)
@@ -412,11 +422,13 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
     plain_ms, _ = timed(plain, steps, max(1, warmup // 2))
     plain.close()
 
-    # learned partition: for each cell-size preset the width model is trained on clouds of
-    # other seeds at that grid and the margin tuned; the best preset is then tuned further
+    # learned partition: for each cell-size preset (the plain search's tuned grid among
+    # them) and both kinds of width model the model is trained on clouds of other seeds at
+    # that setting and the margin tuned; the best setting is then tuned further
     ctx.set_tuning(**base_tuning)
     learned_tuning, model_info = at.autotune_learned(
-        ctx, *wl_args, train=lambda c: train_model(c, cfg, args.scale, rank), **common)
+        ctx, *wl_args, train=lambda c: train_model(c, cfg, args.scale, rank),
+        presets=at.GRID_PRESETS + [at.grid_of(plain_tuning)], **common)
     learned = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=True, **common)
     ms_learned, clocks = timed(learned, steps, warmup, ClockSampler(dev) if headline else None)
     st = rtnn_b200.Stats()
@@ -524,13 +536,16 @@ def run_rtnn(args, rank, world):
     import rtnn_b200
     from rtnn_b200 import build as rb
     rb.build()
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    # one rank per GPU; RTNN_BENCH_BACKEND=gloo lets several ranks share a device (tests:
+    # the ranks' kernels never wait on one another, only the host-side max over ranks does)
+    backend = os.environ.get("RTNN_BENCH_BACKEND", "nccl")
+    dev = int(os.environ.get("LOCAL_RANK", "0")) % max(1, torch.cuda.device_count())
     torch.cuda.set_device(dev)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     ctx = rtnn_b200.Context(dev)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
 

@@ -206,6 +206,12 @@ typedef struct rtnn_tuning {
                                  halving of the search width (0..8; 0: all narrowed widths
                                  in one bucket). Fewer buckets keep tiles spatially tighter,
                                  more keep a tile's widths alike */
+  uint32_t width_model;       /* RTNN_FLAG_LEARNED: 0: a width per query from the model before
+                                 the query sort, queries bucketed by width (one more pass,
+                                 tight boxes); 1: a width per 32-query tile, evaluated by the
+                                 search kernel itself (no extra pass, one box per tile). The
+                                 model is trained for one kind (rtnn_collect_training follows
+                                 this setting) */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);
@@ -255,9 +261,12 @@ rtnn_status rtnn_selftest_wait_timeout(rtnn_ctx* ctx);
  * until the process exits, and shared by all calls: calls whose work overlaps on the GPU
  * race and must be serialised by the caller. Limits: at most RTNN_NOALLOC_MAX_POINTS points
  * and RTNN_NOALLOC_MAX_QUERIES queries (RTNN_ERR_INVALID_ARGUMENT otherwise). The first call
- * on a device looks up the array's device address and should come before any stream
- * capture; that address is kept for the life of the process, so cudaDeviceReset after the
- * first call on a device is not supported. errbuf (optional, errlen bytes) receives a
+ * on a device looks up the array's device address, page-locks a small status block that
+ * is part of the library and caches launch shapes, and should come before any stream
+ * capture; these are kept for the life of the process, so cudaDeviceReset after the first
+ * call on a device is not supported. Later calls do not synchronise the stream: the last
+ * kernel writes the call's status to that block and the call waits for it (at most a
+ * minute, then RTNN_ERR_DEVICE_TIMEOUT). errbuf (optional, errlen bytes) receives a
  * message when the call fails. */
 #define RTNN_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define RTNN_NOALLOC_MAX_POINTS (1u << 18)

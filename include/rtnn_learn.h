@@ -4,15 +4,20 @@
  * The reference picks each partition's launch radius with an analytic rule: grow a box
  * of cells until it holds K+1 points (calcSearchSize, src/optixNSearch/grid.cu:84-211)
  * and take the equal-volume sphere radius of that box (radiusFromMegacell,
- * sort.cpp:262-269; autoBatchingKNN, sort.cpp:271-320). Here the bucket is the search's
- * tile of 32 consecutive (Hilbert-ordered) queries, and a small MLP (6 -> 32 -> 32 -> 1,
- * ReLU) reads the bucket's occupancy histogram (log1p of the points in cell shells 0, 1,
- * 2 around the cell of the tile's box centre, and log(K+1) - log1p(N2)), log(cell / r)
- * and its extent (log1p of the tile box's longest side in cells), and predicts
- * log(largest K-th neighbor distance of the tile's queries / cell). The search kernel
- * evaluates it once per tile and searches the tile at margin * cell * exp(pred), at most
- * r. Results never depend on the model: a query that finds fewer than K neighbors inside
- * its width is searched again wider, finally at the full radius.
+ * sort.cpp:262-269; autoBatchingKNN, sort.cpp:271-320). Here a small MLP (6 -> 32 -> 32
+ * -> 1, ReLU) predicts a bucket's search width from its occupancy histogram (log1p of the
+ * points in cell shells 0, 1, 2, and log(K+1) - log1p(N2)), log(cell / r) and its extent.
+ * Two kinds of bucket, chosen by rtnn_tuning.width_model:
+ *   0  per query: the shells around the query's cell and the query's distance from the
+ *      cell centre; the model predicts log(K-th distance / cell) before the query sort and
+ *      the queries are bucketed by that width (one more pass, tight search boxes);
+ *   1  per tile: the search's tile of 32 consecutive (Hilbert-ordered) queries, shells
+ *      around the cell of the tile box's centre and the box's longest side; the model
+ *      predicts log(largest K-th distance of the tile's queries / cell) and the search
+ *      kernel evaluates it once per tile (no extra pass, one box per tile).
+ * The width is margin * cell * exp(pred), at most r. Results never depend on the model: a
+ * query that finds fewer than K neighbors inside its width is searched again wider,
+ * finally at the full radius.
  *
  * The network is trained on the GPU by hand-written kernels (forward, backward, Adam)
  * on exact K-th distances produced by the plain search. All pointers are device
@@ -38,12 +43,14 @@ uint32_t rtnn_model_size(void);
 rtnn_status rtnn_model_set(rtnn_ctx* ctx, const float* params, uint32_t n);
 rtnn_status rtnn_model_get(rtnn_ctx* ctx, float* params, uint32_t n);
 
-/* Runs the plain search (sorted rows) on one cloud and writes one training sample per
- * tile of that search (the buckets the learned search forms on the same data): the six
- * bucket features (d_feats[t][6]) and the target log(largest K-th neighbor distance of the
- * tile's queries / cell) (d_target[t]); queries with fewer than K neighbors within r do not
- * count, and a tile of only such queries gets log(1.5 r / cell). *n_samples receives the
- * number of tiles, ceil(n_queries / 32); buffers sized for that many samples suffice. */
+/* Runs the plain search (sorted rows) on one cloud and writes training samples for the
+ * kind of model the context's tuning selects (width_model): per query (0), the query's six
+ * features (d_feats[q][6]) and log(K-th distance / cell) (d_target[q]), a query with fewer
+ * than K neighbors within r getting log(1.5 r / cell); or per tile of that search (1), the
+ * tile's features (d_feats[t][6]) and log(largest K-th distance of its queries / cell)
+ * (d_target[t]), queries with fewer than K neighbors within r not counting and a tile of
+ * only such queries getting log(1.5 r / cell). *n_samples receives the sample count:
+ * n_queries, or ceil(n_queries / 32) tiles; buffers sized for n_queries samples suffice. */
 rtnn_status rtnn_collect_training(rtnn_ctx* ctx, const float* d_points, uint64_t n_points,
                                   const float* d_queries, uint64_t n_queries, rtnn_mode mode,
                                   float radius, uint32_t k, float* d_feats, float* d_target,

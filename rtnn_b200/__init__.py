@@ -79,7 +79,7 @@ class Tuning(ctypes.Structure):
                 ("width_margin", ctypes.c_float), ("fallback_passes", ctypes.c_uint32),
                 ("lane_walk_ratio", ctypes.c_float), ("gap_ratio", ctypes.c_float),
                 ("pending_slots", ctypes.c_uint32), ("query_warps", ctypes.c_uint32),
-                ("buckets_per_halving", ctypes.c_float)]
+                ("buckets_per_halving", ctypes.c_float), ("width_model", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -312,11 +312,12 @@ class Context:
         return p
 
     def collect_training(self, points, queries=None, mode="knn", radius=2.0, k=16):
-        """(features [T, 6], targets [T]) as CUDA tensors, one sample per 32-query tile of
-        one plain search (rtnn_collect_training)."""
+        """(features [S, 6], targets [S]) as CUDA tensors from one plain search
+        (rtnn_collect_training): one sample per query, or one per 32-query tile when the
+        context's tuning has width_model = 1."""
         import torch
         nq = points.shape[0] if queries is None else queries.shape[0]
-        cap = max(1, (nq + 31) // 32)
+        cap = max(1, nq if self.tuning().width_model == 0 else (nq + 31) // 32)
         feats = torch.empty((cap, MODEL_FEATURES), dtype=torch.float32, device=points.device)
         tgt = torch.empty((cap,), dtype=torch.float32, device=points.device)
         n = _U64(0)

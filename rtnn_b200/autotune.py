@@ -49,7 +49,7 @@ GRID_PRESETS = [
 # the learned widths are per tile (the search's bucket), so the analytic partition's
 # width buckets (buckets_per_halving) do not apply
 LEARNED_KNOBS = [
-    ("width_margin", [0.9, 1.0, 1.08, 1.15, 1.25]),
+    ("width_margin", [0.8, 0.9, 1.0, 1.08, 1.15, 1.25]),
     ("fallback_passes", [2, 4, 6]),
 ]
 
@@ -158,14 +158,19 @@ def autotune(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radi
     return best
 
 
+WIDTH_MODELS = [0, 1]   # rtnn_tuning.width_model: per query before the sort, per tile in the search
+MARGINS = [0.8, 0.9, 1.0, 1.1, 1.25]
+
+
 def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radius=0.2,
-                     k=32, train=None, presets=None, log=None):
-    """Tuning for the learned partition. The width model's features depend on the grid, so
-    for every cell-size preset the model is trained at that grid (`train(ctx)` collects
-    training data and trains; what it returns is handed back for the chosen preset) and
-    the width margin is tuned; the best preset's model is kept, then the search and
-    learned knobs, which leave the grid alone, are tuned by descent.
-    Returns (tuning, train's result for the chosen preset)."""
+                     k=32, train=None, presets=None, width_models=None, log=None):
+    """Tuning for the learned partition. The width model's features depend on the grid and
+    on the kind of bucket, so for every cell-size preset and both kinds (width_model 0: a
+    width per query before the sort; 1: a width per 32-query tile inside the search) the
+    model is trained at that setting (`train(ctx)` collects training data and trains; what
+    it returns is handed back for the chosen setting) and the width margin is tuned; the
+    fastest setting keeps its model, then the search and learned knobs, which leave the
+    grid alone, are tuned by descent. Returns (tuning, train's result for the chosen one)."""
     import torch
     offsets = np.asarray(offsets, dtype=np.uint64)
     nq = int(offsets[-1]) if queries is None else int(np.asarray(qoffsets)[-1])
@@ -174,18 +179,25 @@ def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="kn
     start = ctx.tuning().as_dict()
     best = None
     for pre in presets if presets is not None else GRID_PRESETS:
-        ctx.set_tuning(**{**start, **pre})
-        info = train(ctx)
-        tun = autotune(ctx, points, offsets, queries, qoffsets,
-                       knobs=[("width_margin", [1.0, 1.1, 1.25])], use_cache=False, log=log, **kw)
-        ms = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
-        if log:
-            log(f"autotune learned preset {pre}: {ms:.3f} ms")
-        if best is None or ms < best[0]:
-            best = (ms, tun, ctx.get_model(), info)
+        for kind in width_models if width_models is not None else WIDTH_MODELS:
+            ctx.set_tuning(**{**start, **pre, "width_model": kind})
+            info = train(ctx)
+            tun = autotune(ctx, points, offsets, queries, qoffsets,
+                           knobs=[("width_margin", MARGINS)], use_cache=False, log=log, **kw)
+            ms = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
+            if log:
+                log(f"autotune learned preset {pre} width_model {kind}: {ms:.3f} ms")
+            if best is None or ms < best[0]:
+                best = (ms, tun, ctx.get_model(), info)
     _, tun, model, info = best
     ctx.set_tuning(**tun)
     ctx.set_model(model)
     tun = autotune(ctx, points, offsets, queries, qoffsets, knobs=SEARCH_KNOBS + LEARNED_KNOBS,
                    use_cache=False, log=log, **kw)
     return tun, info
+
+
+def grid_of(tuning):
+    """The cell-size part of a tuning, as a preset (e.g. the plain search's tuned grid)."""
+    keys = ("cell_ratio", "min_cell_ratio", "points_per_cell", "query_warps")
+    return {n: tuning[n] for n in keys}

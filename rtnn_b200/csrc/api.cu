@@ -56,13 +56,13 @@ void release(DevBuf& b) {
 struct Workspace {
   DevBuf tables, grids, bbox, cells, rank, spts, keys0, keys1, vals0, vals1, sq, qwidth,
       qwidth_in, fbflag, fbnextw, fbpos[2], fbcloud[2], fbwidth[2], hist, scan_state, counters,
-      in_pts, in_qs, out, kth, ppos;
+      in_pts, in_qs, out, kth, ppos, cellsz;
   bool order_in1 = false;   // the last query sort left its permutation in vals1 (else vals0)
   void release_all() {
     for (DevBuf* b : {&tables, &grids, &bbox, &cells, &rank, &spts, &keys0, &keys1, &vals0,
                       &vals1, &sq, &qwidth, &qwidth_in, &fbflag, &fbnextw, &fbpos[0], &fbpos[1],
                       &fbcloud[0], &fbcloud[1], &fbwidth[0], &fbwidth[1], &hist, &scan_state, &counters,
-                      &in_pts, &in_qs, &out, &kth, &ppos})
+                      &in_pts, &in_qs, &out, &kth, &ppos, &cellsz})
       release(*b);
   }
 };
@@ -86,6 +86,7 @@ struct Params {
   uint32_t k;
   uint32_t flags;
   uint32_t fb_passes;   // escalating fallback passes (partitioned searches)
+  uint32_t width_model; // learned widths: 0 per query (before the sort), 1 per tile (in the search)
 };
 
 uint32_t ceil_log2(uint64_t x) {
@@ -102,7 +103,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.1f, 4u, 0.0f, 2.0f, 16u, 2u, 1.0f};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.1f, 4u, 0.0f, 2.0f, 16u, 2u, 1.0f, 0u};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
@@ -261,10 +262,12 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
 
 // narrowed widths with escalation passes: the analytic partition or the learned widths
 bool partitioned(const Params& p) { return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0; }
-// a width per query before the sort (the analytic partition); the learned widths are per
-// tile, computed by the search kernel itself
+bool learned(const Params& p) { return (p.flags & RTNN_FLAG_LEARNED) != 0; }
+// learned widths per 32-query tile, evaluated by the search kernel itself
+bool tile_widths(const Params& p) { return learned(p) && p.width_model == 1; }
+// a width per query before the sort: the analytic partition, or the per-query model
 bool per_query_widths(const Params& p) {
-  return (p.flags & RTNN_FLAG_PARTITION) != 0 && (p.flags & RTNN_FLAG_LEARNED) == 0;
+  return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0 && !tile_widths(p);
 }
 uint32_t level_bits_of(const Params& p) { return per_query_widths(p) ? 4u : 0u; }
 uint32_t key_bits_of(const Shapes& sh, const Params& p) { return sh.key_bits + level_bits_of(p); }
@@ -289,10 +292,8 @@ rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& 
   RTNN_CU(ensure(ws.vals1, Q * 4), "alloc vals");
   RTNN_CU(ensure(ws.sq, Q * 16), "alloc sorted queries");
   if (pr.flags & RTNN_FLAG_REF_LAYOUT) RTNN_CU(ensure(ws.ppos, N * 4), "alloc point positions");
-  if (per_query_widths(pr)) {
-    RTNN_CU(ensure(ws.qwidth, Q * 4), "alloc widths");
-    RTNN_CU(ensure(ws.qwidth_in, Q * 4), "alloc widths");
-  }
+  RTNN_CU(ensure(ws.qwidth_in, Q * 4), "alloc widths");   // also the training features' pass
+  if (per_query_widths(pr)) RTNN_CU(ensure(ws.qwidth, Q * 4), "alloc widths");
   if (partitioned(pr)) {
     for (int i = 0; i < 2; ++i) {
       RTNN_CU(ensure(ws.fbpos[i], Q * 4), "alloc fallback list");
@@ -336,7 +337,8 @@ uint32_t launches_of(const Shapes& sh, const Params& pr, bool reuse_order = fals
 rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr,
                   const float* d_pts, const float* d_qs, int32_t* d_out, cudaStream_t s,
                   cudaEvent_t* ev, uint32_t index_base = 0, bool reuse_order = false,
-                  float* width_out = nullptr) {
+                  float* width_out = nullptr, float* feats_out = nullptr,
+                  float* cellsz_out = nullptr) {
   Counters* ctr = (Counters*)ws.counters.p;
   const bool knn = pr.mode == RTNN_MODE_KNN;
   const rtnn_tuning& tu = c->tuning;
@@ -366,12 +368,13 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
           "scatter");
   if (ev) RTNN_CU(cudaEventRecord(ev[1], s), "event");
 
-  // analytic density buckets: a width per query (caller's order), then the sort key
-  // cloud | bucket of the width | Hilbert index, so each 32-query tile shares one width
-  // band; the learned widths come per tile from the search kernel itself
+  // density buckets: a width per query (caller's order; analytic or the per-query model),
+  // then the sort key cloud | bucket of the width | Hilbert index, so each 32-query tile
+  // shares one width band. Per-tile learned widths come from the search kernel itself.
+  // feats_out: the per-query model's features of every query (training samples).
   const bool part = partitioned(pr);
   const bool pqw = per_query_widths(pr);
-  if (pqw) {
+  if (pqw || feats_out) {
     WidthArgs w{};
     w.t = t;
     w.grids = grids;
@@ -385,7 +388,11 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     w.radius = pr.radius;
     w.need = pr.k + 1;
     w.alpha = 1.24f;   // equal-volume radius of a (2s+2)-cell cube, util.cpp:422-426
+    w.model = (learned(pr) && !tile_widths(pr)) ? (const float*)c->model.p : nullptr;
+    w.margin = tu.width_margin;
     w.qwidth = (float*)ws.qwidth_in.p;
+    w.feats = feats_out;
+    w.cellsz = cellsz_out;
     RTNN_CU(launch_widths(w, c->n_sms, s), "widths");
   }
   // reuse_order (a RTNN_FLAG_KEEP_ORDER plan after its first execute): the permutation of
@@ -419,7 +426,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.spts = (const float4*)ws.spts.p;
   a.sq = (const float4*)ws.sq.p;
   a.qwidth = pqw ? (const float*)ws.qwidth.p : nullptr;
-  a.model = (pr.flags & RTNN_FLAG_LEARNED) ? (const float*)c->model.p : nullptr;
+  a.model = tile_widths(pr) ? (const float*)c->model.p : nullptr;
   a.margin = tu.width_margin;
   a.width_out = width_out;
   a.out = d_out;
@@ -549,7 +556,8 @@ cudaStream_t stream_of(rtnn_ctx* c) { return c->stream ? c->stream : c->own; }
 // search width of every query.
 rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const float* points,
                        const float* queries, int32_t* out, rtnn_stats* stats,
-                       float* width_out = nullptr) {
+                       float* width_out = nullptr, float* feats = nullptr,
+                       float* cellsz = nullptr) {
   cudaStream_t s = stream_of(c);
   const bool dev = (pr.flags & RTNN_FLAG_DEVICE_POINTERS) != 0;
   const bool same = (queries == nullptr);
@@ -578,7 +586,8 @@ rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const fl
   if (sh.N == 0) {
     RTNN_CU(cudaMemsetAsync(d_out, 0xff, out_bytes, s), "fill output");
   } else {
-    st = issue(c, c->ws, sh, pr, d_pts, d_qs, d_out, s, c->ev, 0, false, width_out);
+    st = issue(c, c->ws, sh, pr, d_pts, d_qs, d_out, s, c->ev, 0, false, width_out, feats,
+               cellsz);
     if (st != RTNN_OK) return st;
   }
   if (!dev) RTNN_CU(cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, s), "copy output");
@@ -827,7 +836,7 @@ rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f) ||
       !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f) || t->pending_slots < 8 ||
       t->pending_slots > 256 || t->query_warps > 2 ||
-      !(t->buckets_per_halving >= 0.f && t->buckets_per_halving <= 8.f))
+      !(t->buckets_per_halving >= 0.f && t->buckets_per_halving <= 8.f) || t->width_model > 1)
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
   return RTNN_OK;
@@ -848,7 +857,7 @@ rtnn_status rtnn_search(rtnn_ctx* c, const float* points, uint64_t n_points, con
   if (flags & RTNN_FLAG_LOCAL_INDICES) flags &= ~RTNN_FLAG_LOCAL_INDICES;  // one cloud: same
   cudaSetDevice(c->device);
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
-  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes, c->tuning.width_model};
   return run_search(c, sh, pr, points, queries, out, stats);
 }
 
@@ -870,7 +879,7 @@ rtnn_status rtnn_search_batched(rtnn_ctx* c, const float* points, const uint64_t
   if (sh.N > 0 && !points) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "points is NULL");
   if (sh.Q > 0 && !out) return fail(c, RTNN_ERR_INVALID_ARGUMENT, "out is NULL");
   cudaSetDevice(c->device);
-  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes, c->tuning.width_model};
   st = reserve(c, c->ws, sh, pr);
   if (st != RTNN_OK) return st;
   const uint32_t n_sub = (flags & (RTNN_FLAG_DEVICE_POINTERS | RTNN_FLAG_REF_LAYOUT)) || sh.N == 0
@@ -902,7 +911,8 @@ rtnn_status rtnn_plan_create(rtnn_ctx* c, rtnn_plan** plan, const uint64_t* poin
   if (st == RTNN_OK && (p->sh.N == 0 || p->sh.Q == 0))
     st = fail(c, RTNN_ERR_INVALID_ARGUMENT, "a plan needs at least one point and one query");
   if (st != RTNN_OK) { delete p; return st; }
-  p->pr = Params{mode, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS, c->tuning.fallback_passes};
+  p->pr = Params{mode, radius, k, flags | RTNN_FLAG_DEVICE_POINTERS, c->tuning.fallback_passes,
+                 c->tuning.width_model};
   p->use_graph = use_graph != 0;
   p->keep_order = (flags & RTNN_FLAG_KEEP_ORDER) != 0;
   cudaSetDevice(c->device);
@@ -1023,31 +1033,55 @@ rtnn_status rtnn_collect_training(rtnn_ctx* c, const float* d_points, uint64_t n
   if (n_points == 0 || n_queries == 0) return RTNN_OK;
   cudaSetDevice(c->device);
   cudaStream_t s = stream_of(c);
+  const bool per_tile = c->tuning.width_model == 1;
   RTNN_CU(ensure(c->ws.out, (size_t)n_queries * k * 4), "alloc rows");
   RTNN_CU(ensure(c->ws.kth, n_queries * 4), "alloc kth");
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
-  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes, c->tuning.width_model};
   int32_t* rows = (int32_t*)c->ws.out.p;
-  // the plain search: exact rows, and the tiles (sorted queries) the learned search forms
-  st = run_search(c, sh, pr, d_points, d_queries, rows, nullptr);
-  if (st != RTNN_OK) return st;
   const float* qs = d_queries ? d_queries : d_points;
+  if (per_tile) {
+    // the plain search: exact rows, and the tiles (sorted queries) the learned search forms
+    st = run_search(c, sh, pr, d_points, d_queries, rows, nullptr);
+    if (st != RTNN_OK) return st;
+    RTNN_CU(launch_kth_dist(rows, (uint32_t)n_queries, k, d_points, qs, (float*)c->ws.kth.p, s),
+            "kth");
+    TileSampleArgs a{};
+    a.t = tables_of(c->ws, 1);
+    a.grids = (const CloudGrid*)c->ws.grids.p;
+    a.cells = (const uint32_t*)c->ws.cells.p;
+    a.total_cells = &((const Counters*)c->ws.counters.p)->total_cells;
+    a.sq = (const float4*)c->ws.sq.p;
+    a.kth = (const float*)c->ws.kth.p;
+    a.n_tiles = sh.n_tiles;
+    a.need = k + 1;
+    a.radius = radius;
+    a.feats = d_feats;
+    a.target = d_target;
+    RTNN_CU(launch_tile_samples(a, c->n_sms, s), "tile samples");
+    RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+    *n_samples = sh.n_tiles;
+    return RTNN_OK;
+  }
+  // per query: the plain search writes every query's features and its cloud's cell edge
+  RTNN_CU(ensure(c->ws.cellsz, n_queries * 4), "alloc cell sizes");
+  st = run_search(c, sh, pr, d_points, d_queries, rows, nullptr, nullptr, d_feats,
+                  (float*)c->ws.cellsz.p);
+  if (st != RTNN_OK) return st;
   RTNN_CU(launch_kth_dist(rows, (uint32_t)n_queries, k, d_points, qs, (float*)c->ws.kth.p, s), "kth");
-  TileSampleArgs a{};
-  a.t = tables_of(c->ws, 1);
-  a.grids = (const CloudGrid*)c->ws.grids.p;
-  a.cells = (const uint32_t*)c->ws.cells.p;
-  a.total_cells = &((const Counters*)c->ws.counters.p)->total_cells;
-  a.sq = (const float4*)c->ws.sq.p;
-  a.kth = (const float*)c->ws.kth.p;
-  a.n_tiles = sh.n_tiles;
-  a.need = k + 1;
-  a.radius = radius;
-  a.feats = d_feats;
-  a.target = d_target;
-  RTNN_CU(launch_tile_samples(a, c->n_sms, s), "tile samples");
+  // target = log(kth / cell); queries with < K neighbors inside r get log(1.5 r / cell)
+  std::vector<float> kth(n_queries), cz(n_queries);
+  RTNN_CU(cudaMemcpyAsync(kth.data(), c->ws.kth.p, n_queries * 4, cudaMemcpyDeviceToHost, s), "copy");
+  RTNN_CU(cudaMemcpyAsync(cz.data(), c->ws.cellsz.p, n_queries * 4, cudaMemcpyDeviceToHost, s), "copy");
   RTNN_CU(cudaStreamSynchronize(s), "synchronize");
-  *n_samples = sh.n_tiles;
+  std::vector<float> tgt(n_queries);
+  for (uint64_t i = 0; i < n_queries; ++i) {
+    const float d = kth[i] >= 0.f ? std::max(kth[i], 1e-6f * radius) : 1.5f * radius;
+    tgt[i] = std::log(d / cz[i]);
+  }
+  RTNN_CU(cudaMemcpyAsync(d_target, tgt.data(), n_queries * 4, cudaMemcpyHostToDevice, s), "copy");
+  RTNN_CU(cudaStreamSynchronize(s), "synchronize");
+  *n_samples = n_queries;
   return RTNN_OK;
 }
 
@@ -1065,7 +1099,7 @@ rtnn_status rtnn_query_widths(rtnn_ctx* c, const float* d_points, uint64_t n_poi
   cudaStream_t s = stream_of(c);
   RTNN_CU(ensure(c->ws.out, (size_t)n_queries * k * 4), "alloc rows");
   const Shapes sh = single_shapes(n_points, n_queries, c->tuning);
-  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes};
+  const Params pr{mode, radius, k, flags, c->tuning.fallback_passes, c->tuning.width_model};
   // the first search pass writes the width it searched each query at (per query for the
   // analytic partition, per tile for the learned widths)
   st = run_search(c, sh, pr, d_points, d_queries, (int32_t*)c->ws.out.p, nullptr, d_widths);

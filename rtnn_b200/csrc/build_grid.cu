@@ -79,20 +79,46 @@ __device__ __forceinline__ float warp_max(float v) {
 }
 
 // bbox layout: [3 * n_clouds] ordered mins, then [3 * n_clouds] ordered maxs.
+// Streams the chunk straight from HBM: the AoS float3 input is read as 16-byte words (edge
+// words of the chunk and of an unaligned input fall back to scalars), and float f of the
+// array is component f % 3 of its point, so each thread folds the four floats of a word
+// into the component each belongs to -- no staging through shared memory, no block-wide
+// wait before the reduction. Non-finite coordinates are skipped.
 __global__ void __launch_bounds__(256)
 k_bbox(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, CloudTables t,
        uint32_t* __restrict__ bbox) {
-  __shared__ float s_xyz[kChunk * 3];
   __shared__ float s_red[6][8];
   const ChunkRange r = chunk_range(t.chunk_base, t.point_off, t.n_clouds, blockIdx.x);
-  load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
   float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (uint32_t i = threadIdx.x; i < r.end - r.begin; i += blockDim.x) {
+  const uint64_t f0 = (uint64_t)r.begin * 3, f1 = (uint64_t)r.end * 3;
+  // float f >= f0 of the array is component (f - f0) % 3 (f0 is a point's first float)
+  auto fold = [&](uint64_t f, float v) {
+    const uint32_t c = (uint32_t)(f - f0) % 3u;
+    const bool ok = isfinite(v);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float v = s_xyz[3 * i + a];
-      if (isfinite(v)) { mn[a] = fminf(mn[a], v); mx[a] = fmaxf(mx[a], v); }
+      mn[a] = (ok && c == (uint32_t)a) ? fminf(mn[a], v) : mn[a];
+      mx[a] = (ok && c == (uint32_t)a) ? fmaxf(mx[a], v) : mx[a];
     }
+  };
+  if (aligned) {
+    const uint64_t a0 = f0 & ~3ull;                  // first 16-byte word touching the chunk
+    const uint64_t full_end = total_floats & ~3ull;  // words wholly inside the array
+    const uint64_t nw = (f1 - a0 + 3) >> 2;
+    const float4* w4 = reinterpret_cast<const float4*>(xyz + a0);
+    for (uint64_t w = threadIdx.x; w < nw; w += blockDim.x) {
+      const uint64_t f = a0 + 4 * w;
+      if (f >= f0 && f + 4 <= f1 && f + 4 <= full_end) {
+        const float4 v = __ldg(w4 + w);
+        fold(f, v.x); fold(f + 1, v.y); fold(f + 2, v.z); fold(f + 3, v.w);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (f + i >= f0 && f + i < f1) fold(f + i, __ldg(xyz + f + i));
+      }
+    }
+  } else {
+    for (uint64_t f = f0 + threadIdx.x; f < f1; f += blockDim.x) fold(f, __ldg(xyz + f));
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -217,11 +243,15 @@ k_grid_plan(CloudTables t, const uint32_t* __restrict__ bbox, float radius, floa
   }
 }
 
+// Zeroes the total_cells + 1 counters with 16-byte stores (cells is 16-byte aligned).
 __global__ void k_zero_cells(uint32_t* __restrict__ cells, const Counters* ctr) {
   const uint64_t n = (uint64_t)ctr->total_cells + 1;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    cells[i] = 0u;
+  const uint64_t n4 = n >> 2;
+  uint4* c4 = reinterpret_cast<uint4*>(cells);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t i = tid; i < n4; i += stride) c4[i] = make_uint4(0u, 0u, 0u, 0u);
+  if (tid < (n & 3)) cells[4 * n4 + tid] = 0u;
 }
 
 __device__ __forceinline__ uint32_t point_cell(const CloudGrid& g, float x, float y, float z) {

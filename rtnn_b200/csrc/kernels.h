@@ -129,7 +129,8 @@ constexpr int kNormParams = 2 * kFeatDim + 2;
 constexpr int kTrainParams = kHidden * kFeatDim + kHidden + kHidden * kHidden + kHidden + kHidden + 1;
 constexpr int kModelParams = kNormParams + kTrainParams;
 
-// analytic partition (RTNN_FLAG_PARTITION): a width per query from the box counts
+// a width per query before the sort: the analytic partition (RTNN_FLAG_PARTITION), or the
+// per-query width model (RTNN_FLAG_LEARNED with rtnn_tuning.width_model == 0)
 struct WidthArgs {
   CloudTables t;
   const CloudGrid* grids;
@@ -142,7 +143,11 @@ struct WidthArgs {
   float radius;
   uint32_t need;          // points a width must enclose (K + 1)
   float alpha;            // analytic width = alpha * (s* + 1) * cell
+  const float* model;     // per-query width model (nullptr: analytic)
+  float margin;           // learned width = margin * predicted K-th distance
   float* qwidth;          // out: per query width, caller order (>= radius means full radius)
+  float* feats;           // optional out: [query index][kFeatDim] features (caller order)
+  float* cellsz;          // optional out: [query index] cell edge of the query's cloud
 };
 cudaError_t launch_widths(const WidthArgs& a, int n_sms, cudaStream_t s);
 

@@ -16,12 +16,21 @@
 // In host code the array's name is only a host-side stand-in: its device address is
 // looked up with cudaGetSymbolAddress once per device (with that device current) on the
 // first call made on that device, which is why that first call should come before any
-// stream capture begins. The address is cached for the life of the process, so a
-// cudaDeviceReset after the first call on a device is not supported. Beside a global-mode
-// capture on another thread the caller passes a non-blocking stream: the legacy default
-// stream would wait on the capturing stream and break its capture.
+// stream capture begins. That first call also page-locks a small static status block in
+// host memory (no allocation: the block is part of the library) and caches the search
+// kernels' launch shapes, so that later calls make no call that synchronises the device or
+// could join another thread's capture: the call enqueues its kernels and a last one that
+// writes the device status and a sequence number into the mapped status block, and the
+// host waits for that number (for at most a minute) instead of synchronising the stream.
+// The addresses are cached for the life of the process, so a cudaDeviceReset after the
+// first call on a device is not supported. Beside a global-mode capture on another thread
+// the caller passes a non-blocking stream: the legacy default stream would wait on the
+// capturing stream and break its capture.
+#include <atomic>
+#include <chrono>
 #include <cstring>
 #include <mutex>
+#include <thread>
 
 #include "../../include/rtnn.h"
 #include "kernels.h"
@@ -36,6 +45,51 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void* g_scratch_ptr[kMaxDevices] = {};
 int g_sms[kMaxDevices] = {};
+
+// Completion status of the last call on each device, written by the device through the
+// mapped (page-locked) host block: error and error_info, then seq.
+struct alignas(64) NoallocStatus {
+  volatile uint32_t seq;
+  volatile uint32_t error;
+  volatile uint32_t error_info;
+  uint32_t pad[13];
+};
+alignas(4096) NoallocStatus g_status[kMaxDevices];   // one page
+bool g_status_pinned = false;
+NoallocStatus* g_status_dev[kMaxDevices] = {};   // device view of g_status[dev]
+uint32_t g_seq[kMaxDevices] = {};
+// search blocks per SM for every K (index k - 1) and mode, cached at set-up
+int g_bps[kMaxDevices][2][RTNN_MAX_K] = {};
+constexpr double kWaitSeconds = 60.0;
+
+__global__ void k_noalloc_publish(const Counters* ctr, NoallocStatus* st, uint32_t seq) {
+  st->error = ctr ? ctr->error : 0u;
+  st->error_info = ctr ? ctr->error_info : 0u;
+  __threadfence_system();
+  st->seq = seq;
+}
+
+// Enqueues the status write and waits (bounded) for it to arrive in host memory.
+cudaError_t publish_and_wait(int dev, const Counters* ctr, cudaStream_t s, bool* timed_out) {
+  *timed_out = false;
+  const uint32_t seq = ++g_seq[dev];
+  k_noalloc_publish<<<1, 1, 0, s>>>(ctr, g_status_dev[dev], seq);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const auto t0 = std::chrono::steady_clock::now();
+  while (g_status[dev].seq != seq) {
+    std::this_thread::yield();
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > kWaitSeconds) {
+      // a kernel that faulted never lets the status through: report its error if it did
+      const cudaError_t q = cudaStreamQuery(s);
+      if (q != cudaSuccess && q != cudaErrorNotReady) return q;
+      *timed_out = true;
+      return cudaSuccess;
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return cudaSuccess;
+}
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -79,14 +133,9 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
   }
   if (n_queries == 0) return RTNN_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  if (n_points == 0) {
-    cudaError_t e = cudaMemsetAsync(d_out, 0xff, (size_t)n_queries * k * 4, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) { set_msg(errbuf, errlen, cudaGetErrorString(e)); return RTNN_ERR_CUDA; }
-    return RTNN_OK;
-  }
 
-  // set-up, once per device: the scratch array's device address, SM count, kernel attributes
+  // set-up, once per device: the scratch array's device address, SM count, kernel
+  // attributes, the page-locked status block and the search kernels' launch shapes
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
@@ -101,6 +150,23 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
       cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
       if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev);
       if (e == cudaSuccess) e = search_prepare(dev);
+      if (e == cudaSuccess && !g_status_pinned) {
+        e = cudaHostRegister(g_status, sizeof(g_status),
+                             cudaHostRegisterPortable | cudaHostRegisterMapped);
+        if (e == cudaSuccess) g_status_pinned = true;
+      }
+      if (e == cudaSuccess) {
+        void* dp = nullptr;
+        e = cudaHostGetDevicePointer(&dp, &g_status[dev], 0);
+        g_status_dev[dev] = (NoallocStatus*)dp;
+      }
+      for (int knn = 0; knn < 2 && e == cudaSuccess; ++knn)
+        for (uint32_t kk = 1; kk <= RTNN_MAX_K; ++kk) {
+          uint32_t pend = 16;
+          int wpb = 4;
+          fit_search_shape(kk, 16u, 4, &pend, &wpb);
+          g_bps[dev][knn][kk - 1] = search_blocks_per_sm(knn != 0, kk, pend, wpb);
+        }
       if (e != cudaSuccess || !ptr) {
         cudaGetLastError();
         set_msg(errbuf, errlen, e != cudaSuccess ? cudaGetErrorString(e) : "scratch address is NULL");
@@ -111,6 +177,17 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
     base = (unsigned char*)g_scratch_ptr[dev];
   }
   const int n_sms = g_sms[dev];
+  bool timed_out = false;
+  if (n_points == 0) {
+    cudaError_t e = cudaMemsetAsync(d_out, 0xff, (size_t)n_queries * k * 4, s);
+    if (e == cudaSuccess) e = publish_and_wait(dev, nullptr, s, &timed_out);
+    if (e != cudaSuccess) { set_msg(errbuf, errlen, cudaGetErrorString(e)); return RTNN_ERR_CUDA; }
+    if (timed_out) {
+      set_msg(errbuf, errlen, "rtnn_search_noalloc: the device did not finish within a minute");
+      return RTNN_ERR_DEVICE_TIMEOUT;
+    }
+    return RTNN_OK;
+  }
 
   // fixed tuning: cell = r/2, at most 2 cells per point (+64), plain (no partition)
   const uint64_t N = n_points, Q = n_queries;
@@ -191,22 +268,25 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
     a.pass = kPassMain;
     int wpb = 4;
     fit_search_shape(k, 16u, 4, &a.pending, &wpb);
-    const uint64_t blocks = (uint64_t)n_sms * search_blocks_per_sm(knn, k, a.pending, wpb);
+    const uint64_t blocks = (uint64_t)n_sms * g_bps[dev][knn ? 1 : 0][k - 1];
     const uint64_t need = (n_tiles + wpb - 1) / wpb;
     e = launch_search(knn, a, (unsigned)(blocks < need ? blocks : need), wpb, s);
   }
-  Counters h;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = publish_and_wait(dev, ctr, s, &timed_out);
   if (e != cudaSuccess) {
     set_msg(errbuf, errlen, cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? RTNN_ERR_OUT_OF_MEMORY : RTNN_ERR_CUDA;
   }
-  if (h.error == kErrScanTimeout) {
+  if (timed_out) {
+    set_msg(errbuf, errlen, "rtnn_search_noalloc: the device did not finish within a minute");
+    return RTNN_ERR_DEVICE_TIMEOUT;
+  }
+  const uint32_t error = g_status[dev].error;
+  if (error == kErrScanTimeout) {
     set_msg(errbuf, errlen, "scan look-back gave up waiting");
     return RTNN_ERR_DEVICE_TIMEOUT;
   }
-  if (h.error != 0) {
+  if (error != 0) {
     set_msg(errbuf, errlen, "device consistency check failed");
     return RTNN_ERR_INTERNAL;
   }

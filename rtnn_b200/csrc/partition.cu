@@ -106,24 +106,30 @@ __device__ __forceinline__ float mlp_forward_norm_x2(const MlpView& m, const flo
 }
 
 // The three box counts N_0..N_2 in one pass over the 25 rows of the 5 x 5 x 5 box: the six
-// offsets a row needs (x - 2 .. x + 3) sit in one or two 32-byte sectors.
+// offsets a row needs (x - 2 .. x + 3) sit in one or two 32-byte sectors. The 25 rows are
+// unrolled and every load is issued unconditionally (a row outside the grid reads the
+// query's own row and counts nothing), so the ~70 loads of a query are in flight together
+// instead of one row after another.
 static_assert(kShells == 3, "box_counts3 counts three shells");
 __device__ __forceinline__ void box_counts3(const CloudGrid& g, const uint32_t* cells, int cx,
                                             int cy, int cz, uint32_t* N) {
   const int x0 = max(cx - 2, 0), x1 = min(cx + 2, g.dx - 1);
   const int i0 = max(cx - 1, 0), i1 = min(cx + 1, g.dx - 1);
+  const uint32_t* base = cells + g.cell_base;
   uint32_t n0 = 0, n1 = 0, n2 = 0;
+#pragma unroll
   for (int dz = -2; dz <= 2; ++dz) {
-    const int z = cz + dz;
-    if (z < 0 || z >= g.dz) continue;
+#pragma unroll
     for (int dy = -2; dy <= 2; ++dy) {
-      const int y = cy + dy;
-      if (y < 0 || y >= g.dy) continue;
+      const int z = cz + dz, y = cy + dy;
+      const bool in = z >= 0 && z < g.dz && y >= 0 && y < g.dy;
       const uint32_t* row =
-          cells + g.cell_base + ((uint32_t)z * (uint32_t)g.dy + (uint32_t)y) * (uint32_t)g.dx;
-      n2 += __ldg(row + x1 + 1) - __ldg(row + x0);
+          base + ((uint32_t)(in ? z : cz) * (uint32_t)g.dy + (uint32_t)(in ? y : cy)) * (uint32_t)g.dx;
+      const uint32_t c2 = __ldg(row + x1 + 1) - __ldg(row + x0);
+      n2 += in ? c2 : 0u;
       if (dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
-        n1 += __ldg(row + i1 + 1) - __ldg(row + i0);
+        const uint32_t c1 = __ldg(row + i1 + 1) - __ldg(row + i0);
+        n1 += in ? c1 : 0u;
         if (dy == 0 && dz == 0) n0 += __ldg(row + cx + 1) - __ldg(row + cx);
       }
     }
@@ -144,8 +150,18 @@ __device__ __forceinline__ float wmax_f(float v) {
   return v;
 }
 
+// A width per query: the box counts around its cell, then the analytic rule or the
+// per-query width model. Per-query model features:
+//   f0..f2 log1p of the points in cell shells 0, 1, 2 around the query's cell,
+//   f3     log(K + 1) - log1p(N2),
+//   f4     log(cell / r),
+//   f5     the query's distance from its cell's centre, in cells (at most 1).
 __global__ void __launch_bounds__(256)
 k_widths(WidthArgs a) {
+  __shared__ float s_model[kModelParams];
+  __shared__ __align__(8) float s_w2p[kHidden * kHidden];   // W2, unit pairs interleaved
+  if (a.model) load_model_smem(a.model, s_model, s_w2p);
+  const MlpView mv = mlp_view(s_model);
   const uint32_t total_cells = a.total_cells ? *a.total_cells : 0u;
   // queries that are the points are taken in cell order (neighbouring threads read the
   // same cell rows); only the points placed in cells are there, the rest keep no width
@@ -174,11 +190,34 @@ k_widths(WidthArgs a) {
     const int cz = clamp_cell(cell_coord_f(qz, g.oz, g.inv_cell), g.dz);
     uint32_t N[kShells];
     box_counts3(g, a.cells, cx, cy, cz, N);
-    float w = INFINITY;
+    // offset of the query from its cell's centre, in cells (0 .. 0.87)
+    const float ox = (qx - g.ox) * g.inv_cell - ((float)cx + 0.5f);
+    const float oy = (qy - g.oy) * g.inv_cell - ((float)cy + 0.5f);
+    const float oz = (qz - g.oz) * g.inv_cell - ((float)cz + 0.5f);
+    float feat[kFeatDim];
+    feat[0] = log1pf((float)N[0]);
+    feat[1] = log1pf((float)(N[1] - N[0]));
+    feat[2] = log1pf((float)(N[2] - N[1]));
+    feat[3] = logf((float)a.need) - log1pf((float)N[2]);
+    feat[4] = logf(g.cell / a.radius);
+    feat[5] = fminf(sqrtf(ox * ox + oy * oy + oz * oz), 1.f);
+    float w;
+    if (a.model) {
+      const float o = mlp_forward_norm_x2(mv, s_w2p, feat);
+      const float y = fmaf(o, mv.out_std, mv.out_mean);
+      w = a.margin * g.cell * expf(fminf(y, 30.f));
+    } else {
+      w = INFINITY;
 #pragma unroll
-    for (int s = 0; s < kShells; ++s)
-      if (w == INFINITY && N[s] >= a.need) w = a.alpha * (float)(s + 1) * g.cell;
+      for (int s = 0; s < kShells; ++s)
+        if (w == INFINITY && N[s] >= a.need) w = a.alpha * (float)(s + 1) * g.cell;
+    }
     a.qwidth[i] = (w < a.radius) ? w : a.radius;
+    if (a.feats) {
+#pragma unroll
+      for (int f = 0; f < kFeatDim; ++f) a.feats[(size_t)i * kFeatDim + f] = feat[f];
+    }
+    if (a.cellsz) a.cellsz[i] = g.cell;
   }
 }
 

@@ -341,8 +341,10 @@ __device__ __forceinline__ float learned_tile_width(const SearchArgs& a, uint32_
 // KC > 0: the search for K == KC compiled in (the reference compiles its K in,
 // camera.cu:66-72, CMakeLists.txt:58-61), with kFixedPending appended-hit slots, so the
 // column length and every heap loop bound are constants; KC == 0: any K and slot count.
+// Small compiled K (short result columns, so shared memory allows more resident warps):
+// registers are capped so that 6 blocks of 4 warps fit an SM.
 template <bool KNN, int KC>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, (KC > 0 && KC <= 16) ? 3 : 2)
 k_search(SearchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;

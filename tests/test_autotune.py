@@ -16,7 +16,7 @@ from rtnn_b200 import autotune as at
 DEFAULT = dict(cell_ratio=0.5, min_cell_ratio=0.0625, points_per_cell=0.0, cell_budget=16.0,
                warps_per_block=4, blocks_per_sm=0, width_margin=1.1, fallback_passes=4,
                lane_walk_ratio=0.0, gap_ratio=2.0, pending_slots=16, query_warps=2,
-               buckets_per_halving=1.0)
+               buckets_per_halving=1.0, width_model=0)
 
 
 class _Tuning(dict):
@@ -53,7 +53,8 @@ class FakeCtx:
         ok = (0 < kw["cell_ratio"] <= 64 and 0 < kw["min_cell_ratio"] <= kw["cell_ratio"] and
               kw["points_per_cell"] >= 0 and 1 <= kw["warps_per_block"] <= 8 and
               8 <= kw["pending_slots"] <= 256 and kw["query_warps"] <= 2 and
-              kw["fallback_passes"] <= 6 and 0 <= kw["buckets_per_halving"] <= 8)
+              kw["fallback_passes"] <= 6 and 0 <= kw["buckets_per_halving"] <= 8 and
+              kw["width_model"] <= 1)
         if not ok:
             self.rejected += 1
             raise rtnn_b200.RtnnError(1, "tuning values out of range")
@@ -127,25 +128,33 @@ def test_cache_skips_the_search(tmp_path, monkeypatch):
 
 
 def test_learned_keeps_the_model_of_the_winning_preset():
-    # the model trained at a grid only pays at that grid; the second preset's grid with
-    # its own model is fastest, and its margin optimum is 1.25
+    # the model trained at a grid and bucket kind only pays there; the second preset's grid
+    # with per-tile widths and its own model is fastest, and its margin optimum is 1.25
     def cost(t, model):
         c = 1.0 + abs(t["width_margin"] - 1.25)
-        if model != ("model", t["cell_ratio"]):
+        if model != ("model", t["cell_ratio"], t["width_model"]):
             c += 10.0
+        c += 0.0 if t["width_model"] == 1 else 0.5
         return c + (0.0 if t["cell_ratio"] == 0.25 else 1.0)
 
     ctx = FakeCtx(cost)
     trained = []
 
     def train(c):
-        c.set_model(("model", c.tun["cell_ratio"]))
-        trained.append(c.tun["cell_ratio"])
-        return {"preset": c.tun["cell_ratio"]}
+        c.set_model(("model", c.tun["cell_ratio"], c.tun["width_model"]))
+        trained.append((c.tun["cell_ratio"], c.tun["width_model"]))
+        return {"preset": c.tun["cell_ratio"], "kind": c.tun["width_model"]}
 
     tun, info = at.autotune_learned(ctx, POINTS, OFFSETS, mode="knn", radius=0.2, k=8,
                                     train=train)
-    assert trained == [p["cell_ratio"] for p in at.GRID_PRESETS]
-    assert tun["cell_ratio"] == 0.25 and info == {"preset": 0.25}
-    assert ctx.model == ("model", 0.25) and ctx.tun == tun
+    assert trained == [(p["cell_ratio"], kind) for p in at.GRID_PRESETS for kind in (0, 1)]
+    assert tun["cell_ratio"] == 0.25 and tun["width_model"] == 1
+    assert info == {"preset": 0.25, "kind": 1}
+    assert ctx.model == ("model", 0.25, 1) and ctx.tun == tun
     assert tun["width_margin"] == 1.25
+
+
+def test_grid_of_takes_the_cell_settings():
+    t = dict(DEFAULT, cell_ratio=0.125, points_per_cell=0.125, min_cell_ratio=0.01, query_warps=1)
+    assert at.grid_of(t) == dict(cell_ratio=0.125, min_cell_ratio=0.01, points_per_cell=0.125,
+                                 query_warps=1)

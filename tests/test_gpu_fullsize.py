@@ -4,9 +4,10 @@ At full size the oracle cannot search every query in seconds, so each workload i
 on a seeded subset of 1,000 queries, row for row (rows sorted by (FP32 distance, index))
 against the oracle's brute force over the query's own cloud, and the same subset is run
 through the reference's own check (check.cpp:20-101 KNN, :103-139 radius, compiled into
-oracle/_ref/refcheck). Every workload runs twice, on the plain grid and on the learned
-partition with the tuning the benchmark settles on (fine cells, one warp per query for
-the escalation passes); the two must agree on every row.
+oracle/_ref/refcheck). Every workload runs on the plain grid and on the learned partition
+(a width per query, and a width per tile) with the tuning the benchmark settles on for the
+multi-cloud workload (fine cells, one warp per query for the escalation passes); all must
+agree on every row.
 
   surfaces   10,000,000 surface points, queries = points, KNN K = 16, r = 2
   multicloud 4,096 clouds (54.8 M points), queries = own points, KNN K = 32, r = 0.2
@@ -32,17 +33,21 @@ THREADS = os.cpu_count() or 1
 
 
 def _search_both(ctx, name, tp, offsets):
-    """(plain rows, learned rows, learned stats) as CUDA tensors, rows sorted."""
+    """(plain rows, [learned rows per width model], learned stats) as CUDA tensors, rows
+    sorted; the learned search runs with a width per query and with a width per tile."""
     import torch
     cfg = wl.CONFIGS[name]
     kw = dict(mode=cfg["mode"], radius=cfg["radius"], k=cfg["k"], sorted_rows=True)
     base = ctx.tuning().as_dict()
     plain = ctx.search_batched(tp, offsets, **kw)
-    ctx.set_tuning(**TUNED)
-    wl.train_width_model(ctx, name, epochs=8, count=4 if name != "knn_multicloud_4096" else 48)
-    st = rtnn_b200.Stats()
-    learned = ctx.search_batched(tp, offsets, learned=True, stats=st, **kw)
-    torch.cuda.synchronize()
+    learned, st = [], None
+    for kind in (0, 1):
+        ctx.set_tuning(**{**base, **TUNED, "width_model": kind})
+        wl.train_width_model(ctx, name, epochs=8,
+                             count=4 if name != "knn_multicloud_4096" else 48)
+        st = rtnn_b200.Stats()
+        learned.append(ctx.search_batched(tp, offsets, learned=True, stats=st, **kw))
+        torch.cuda.synchronize()
     ctx.set_tuning(**base)
     return plain, learned, st
 
@@ -74,7 +79,8 @@ def _run(ctx, name, points, offsets):
     import torch
     tp = torch.from_numpy(points).cuda()
     plain, learned, st = _search_both(ctx, name, tp, offsets)
-    assert torch.equal(plain, learned), "plain and learned rows differ"
+    for kind, rows in enumerate(learned):
+        assert torch.equal(plain, rows), f"plain and learned rows differ (width model {kind})"
     assert st.n_queries == points.shape[0]
     idx = np.sort(np.random.default_rng(12345).choice(points.shape[0], SUBSET, replace=False))
     sub = plain[torch.from_numpy(idx).cuda()].cpu().numpy()

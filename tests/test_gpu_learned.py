@@ -83,11 +83,21 @@ def _cloud(seed, n=200_000):
     return wl.surfaces(n=n, n_spheres=4, n_quads=4, box=100.0, seed=seed)
 
 
-def _train(ctx, mode="knn", r=2.0, k=16, seeds=range(20, 26), epochs=15):
+@pytest.fixture(params=[0, 1], ids=["per_query", "per_tile"])
+def kind(request, ctx):
+    """The width model's bucket: 0 a width per query before the sort, 1 a width per tile
+    inside the search (rtnn_tuning.width_model); restored after the test."""
+    base = ctx.tuning().as_dict()
+    ctx.set_tuning(**{**base, "width_model": request.param})
+    yield request.param
+    ctx.set_tuning(**base)
+
+
+def _train(ctx, mode="knn", r=2.0, k=16, seeds=range(20, 26), epochs=15, n=200_000):
     import torch
     fs, ts = [], []
     for s in seeds:
-        p = torch.from_numpy(_cloud(s)).cuda()
+        p = torch.from_numpy(_cloud(s, n)).cuda()
         f, t = ctx.collect_training(p, None, mode, r, k)
         fs.append(f)
         ts.append(t)
@@ -95,14 +105,15 @@ def _train(ctx, mode="knn", r=2.0, k=16, seeds=range(20, 26), epochs=15):
     t = torch.cat(ts)
     perm = torch.randperm(f.shape[0], device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
     return ctx.train_model(f[perm].contiguous(), t[perm].contiguous(), epochs=epochs,
-                           batch=8192, lr=3e-3, seed=1)
+                           batch=8192 if ctx.tuning().width_model == 0 else 1024, lr=3e-3, seed=1)
 
 
-def test_training_reduces_loss_and_learned_search_is_exact(ctx):
+def test_training_reduces_loss_and_learned_search_is_exact(ctx, kind):
     import torch
-    losses = _train(ctx)
+    losses = _train(ctx, epochs=15 if kind == 0 else 40)
     # normalised targets: predicting their mean scores 0.5; training must beat it and improve
-    assert losses[-1] < losses[0] and losses[-1] < 0.45, losses
+    # (the per-tile target, the largest K-th distance of 32 queries, is the noisier one)
+    assert losses[-1] < losses[0] and losses[-1] < (0.45 if kind == 0 else 0.49), losses
     P = ctx.get_model()
     assert np.isfinite(P).all()
     p = _cloud(2, 60_000)
@@ -116,7 +127,7 @@ def test_training_reduces_loss_and_learned_search_is_exact(ctx):
     assert np.array_equal(ctx.get_model(), P)
 
 
-def test_escalating_fallback_stays_exact(ctx):
+def test_escalating_fallback_stays_exact(ctx, kind):
     """Widths far too small force queries through every doubling pass and the final
     full-radius pass; rows stay identical to the oracle."""
     import torch
@@ -153,6 +164,31 @@ def test_learned_widths_are_tighter_than_analytic(ctx):
     assert fb_rate < 0.25
 
 
+def test_width_features_match_oracle_box_counts(ctx):
+    """The per-query model's shell-count features (N_0..N_2 box counts around a query's
+    cell) equal the oracle's counts on the same grid (cell and origin from the search)."""
+    import torch
+    p = wl.uniform_cube(20000, 30.0, seed=12)
+    tp = torch.from_numpy(p).cuda()
+    st = rtnn_b200.Stats()
+    ctx.search(tp, None, "knn", 2.0, 16, partition=True, stats=st)
+    f, _ = ctx.collect_training(tp, None, "knn", 2.0, 16)
+    f = f.cpu().numpy()
+    assert f.shape == (p.shape[0], rtnn_b200.MODEL_FEATURES)
+    cell = np.float32(st.cell_size)
+    dims = np.array(list(st.grid_dims))
+    o = p.min(0).astype(np.float32)
+    inv = np.float32(1) / cell
+    ci = np.clip(np.floor((p - o) * inv), 0, dims - 1).astype(np.int64)
+    counts = np.zeros(dims[::-1], dtype=np.uint32)
+    np.add.at(counts, (ci[:, 2], ci[:, 1], ci[:, 0]), 1)
+    for i in range(0, p.shape[0], 37):
+        N = oracle.box_counts(counts, *ci[i], shells=3).astype(np.float64)
+        exp = np.log1p([N[0], N[1] - N[0], N[2] - N[1]])
+        assert np.allclose(f[i, [0, 1, 2]], exp, atol=1e-5), (i, f[i], N)
+        assert abs(f[i, 3] - (np.log(17.0) - np.log1p(N[2]))) <= 1e-5
+
+
 def test_tile_features_and_targets_match_the_oracle(ctx):
     """One training sample per 32-query tile of the plain search: the shell-count features
     (N_0..N_2 box counts around the cell of the tile box's centre) equal the oracle's counts
@@ -165,7 +201,12 @@ def test_tile_features_and_targets_match_the_oracle(ctx):
     tp = torch.from_numpy(p).cuda()
     st = rtnn_b200.Stats()
     ctx.search(tp, None, "knn", r, k, stats=st)
-    f, t = ctx.collect_training(tp, None, "knn", r, k)
+    base = ctx.tuning().as_dict()
+    ctx.set_tuning(**{**base, "width_model": 1})
+    try:
+        f, t = ctx.collect_training(tp, None, "knn", r, k)
+    finally:
+        ctx.set_tuning(**base)
     _, qo = ctx.layout(n, n)   # the sorted order of that plain search: tile t = rows 32t..
     f, t = f.cpu().numpy(), t.cpu().numpy()
     assert f.shape == ((n + 31) // 32, rtnn_b200.MODEL_FEATURES) and t.shape == (f.shape[0],)
@@ -200,12 +241,22 @@ def test_tile_features_and_targets_match_the_oracle(ctx):
 
 
 def test_learned_tile_widths_cover_most_queries(ctx):
-    """The widths the learned search uses are one per tile (bucket): every query of a tile
-    gets the same width, below r where the data is dense, and the share of queries that
-    need the wider fallback stays small."""
+    """With per-tile widths the search uses one width per tile (bucket): every query of a
+    tile gets the same width, below r where the data is dense (clouds four times denser
+    than the other tests', about 0.8 r for the 16th neighbor), and the share of queries
+    that need the wider fallback stays small."""
     import torch
-    _train(ctx)
-    p = torch.from_numpy(_cloud(4)).cuda()
+    base = ctx.tuning().as_dict()
+    ctx.set_tuning(**{**base, "width_model": 1})
+    try:
+        _tile_widths_check(ctx, torch)
+    finally:
+        ctx.set_tuning(**base)
+
+
+def _tile_widths_check(ctx, torch):
+    _train(ctx, epochs=40, n=800_000, seeds=range(20, 23))
+    p = torch.from_numpy(_cloud(4, 800_000)).cuda()
     w = ctx.query_widths(p, None, "knn", 2.0, 16, learned=True).cpu().numpy()
     _, qo = ctx.layout(p.shape[0], p.shape[0])
     ws = w[qo.astype(np.int64)]

@@ -75,3 +75,27 @@ def test_two_gloo_ranks_weak_scaling():
     assert hits0 > 0 and hits1 > 0
     # whole-job throughput counts both ranks' queries
     assert thr0 == pytest.approx(2 * g0[0][1] / (max0 * 1e-3))
+
+
+@pytest.mark.gpu
+def test_bench_two_ranks_run_the_cuda_path(tmp_path):
+    """bench.py under torchrun with two ranks sharing the one GPU (gloo for the host-side
+    max over ranks): every rank runs the library's CUDA search on its own instance, and
+    rank 0 prints one line with the job throughput of both ranks."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {**os.environ, "RTNN_BENCH_BACKEND": "gloo",
+           "RTNN_AUTOTUNE_CACHE": str(tmp_path / "autotune.json")}
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+           os.path.join(root, "bench.py"), "--gpus", "2", "--steps", "2", "--warmup", "3",
+           "--scale", "0.005", "--no-other-workloads", "--no-e2e", "--cpu-seconds", "1"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=root, env=env)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["value"] > 0 and d["identical_sets"] is True
+    assert d["gpu_launches"] > 0 and d["cpu_baseline"] is None   # the CPU sample is N=1 only
