@@ -35,19 +35,39 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per query of the main search pass, from the ncu capture in
-# profiles/k_search_knn_multicloud_scale0.1.md (1,102 MB for 5.25 M queries), scaled by
+# profiles/kernels_knn_multicloud_scale0.3.md (3,613 MB for 16.28 M queries), scaled by
 # queries to a full launch; only known for the default workload.
-TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 210.0}
+TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 222.0}
 # Warp instructions per query of the first search pass (smsp__inst_executed.sum over the
-# queries in the same capture: 5.141e9 for 5.25 M queries). The search is bound by
-# instruction issue, not DRAM, so the bench also reports the issue rate this implies.
-INST_PER_QUERY = {"knn_multicloud_4096": 979.0}
+# queries in the capture of profiles/k_search_knn_multicloud_scale0.1.md with K = 32
+# compiled in: 4.958e9 for 5.25 M queries). The search is bound by instruction issue, not
+# DRAM, so the bench also reports the issue rate this implies.
+INST_PER_QUERY = {"knn_multicloud_4096": 944.0}
 # Per-kernel ncu figures of one learned step plus one width-model training step of the
-# default workload at scale 0.1 (409 clouds, 5,250,132 points = queries), from the capture
-# summarised in profiles/kernels_knn_multicloud_scale0.1.md (gpu__time_duration.sum,
+# default workload at scale 0.3 (1,228 clouds, 16,276,803 points = queries), from the
+# capture summarised in profiles/kernels_knn_multicloud_scale0.3.md (gpu__time_duration.sum,
 # dram__bytes_read.sum + dram__bytes_write.sum; times are cold-cache and serialised):
-# kernel -> (launches, total us, DRAM bytes, algorithmic bytes per unit, unit).
-KERNEL_PROFILE = {"knn_multicloud_4096": {"units": 5250132, "kernels": {}}}
+# kernel -> (launches, total us, DRAM bytes, algorithmic bytes per unit, unit); 0 where the
+# kernel's work is not counted in bytes (per short query, or training samples).
+KERNEL_PROFILE = {"knn_multicloud_4096": {"units": 16276803, "kernels": {
+        "k_bbox": (1, 82.5, 199035648, 12, "point"),
+        "k_grid_plan": (1, 11.4, 49920, 0, "point"),
+        "k_zero_cells": (1, 95.0, 498782208, 34, "point"),
+        "k_count": (1, 213.2, 477608960, 16, "point"),
+        "k_scan_excl": (9, 558.6, 1185266432, 68.8, "point"),
+        "k_scatter": (1, 262.5, 798515456, 36, "point"),
+        "k_widths": (1, 1928.4, 748663040, 20, "query"),
+        "k_query_keys<unsigned long>": (1, 293.4, 358462720, 20, "query"),
+        "k_radix_hist<unsigned long>": (5, 257.4, 664676608, 40, "query"),
+        "k_radix_scatter<unsigned long>": (5, 736.4, 1682764288, 116, "query"),
+        "k_gather_queries": (1, 209.9, 659371520, 32, "query"),
+        "k_search<1, 32>": (1, 22250.3, 3612505088, 160, "query"),
+        "k_compact_fallback": (3, 103.5, 111876352, 8, "query"),
+        "k_search_q<1, 32>": (3, 3392.6, 2517571840, 0, "query"),
+        "k_mlp_loss_grad": (1, 219.5, 836096, 0, "sample"),
+        "k_mlp_adam": (1, 6.1, 30208, 0, "sample"),
+        "k_mlp_forward": (1, 12.0, 306432, 0, "sample"),
+}}}
 
 
 def kernel_rooflines(workload):
@@ -413,7 +433,6 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
 
     common = dict(mode=cfg["mode"], radius=cfg["radius"], k=K)
     wl_args = (tp, cfg["offsets"], tq, cfg["qoffsets"])
-    base_tuning = ctx.tuning().as_dict()
 
     # the plain grid search (full radius for every query), with its own best tuning
     plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, presets=at.GRID_PRESETS,
@@ -422,10 +441,11 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
     plain_ms, _ = timed(plain, steps, max(1, warmup // 2))
     plain.close()
 
-    # learned partition: for each cell-size preset (the plain search's tuned grid among
-    # them) and both kinds of width model the model is trained on clouds of other seeds at
-    # that setting and the margin tuned; the best setting is then tuned further
-    ctx.set_tuning(**base_tuning)
+    # learned partition: starting from the plain search's tuned settings, for each
+    # cell-size preset (the plain search's own grid among them) and both kinds of width
+    # model the model is trained on clouds of other seeds at that setting and the margin
+    # tuned; the best setting is then tuned further
+    ctx.set_tuning(**plain_tuning)
     learned_tuning, model_info = at.autotune_learned(
         ctx, *wl_args, train=lambda c: train_model(c, cfg, args.scale, rank),
         presets=at.GRID_PRESETS + [at.grid_of(plain_tuning)], **common)
@@ -556,7 +576,7 @@ def run_rtnn(args, rank, world):
     roofline = m["roofline"]
     roofline.update({"traffic": (round(TRAFFIC_PER_QUERY[args.workload] * Q)
                                  if args.workload in TRAFFIC_PER_QUERY else None),
-                     "traffic_scope": "main search pass, ncu at scale 0.1 scaled by queries"})
+                     "traffic_scope": "main search pass, ncu at scale 0.3 scaled by queries"})
     mhz = (m["clocks"] or {}).get("sm_mhz") or (m["clocks"] or {}).get("sm_max_mhz")
     if args.workload in INST_PER_QUERY and mhz and m["ms_main"] > 0:
         sms = torch.cuda.get_device_properties(dev).multi_processor_count

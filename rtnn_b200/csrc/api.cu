@@ -351,7 +351,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   uint32_t* cells = (uint32_t*)ws.cells.p;
   CloudGrid* grids = (CloudGrid*)ws.grids.p;
 
-  RTNN_CU(launch_bbox(d_pts, sh.N, ap, t, sh.n_chunks, (uint32_t*)ws.bbox.p, s), "bbox");
+  RTNN_CU(launch_bbox(d_pts, sh.N, ap, t, sh.n_chunks, (uint32_t*)ws.bbox.p, c->n_sms, s), "bbox");
   RTNN_CU(launch_grid_plan(t, (const uint32_t*)ws.bbox.p, pr.radius, tu.cell_ratio,
                            tu.min_cell_ratio, tu.points_per_cell, sh.cell_budget, sh.order_bits,
                            sh.cell_capacity, grids, ctr, s),

@@ -79,47 +79,15 @@ __device__ __forceinline__ float warp_max(float v) {
 }
 
 // bbox layout: [3 * n_clouds] ordered mins, then [3 * n_clouds] ordered maxs.
-// Streams the chunk straight from HBM: the AoS float3 input is read as 16-byte words (edge
-// words of the chunk and of an unaligned input fall back to scalars), and float f of the
-// array is component f % 3 of its point, so each thread folds the four floats of a word
-// into the component each belongs to -- no staging through shared memory, no block-wide
-// wait before the reduction. Non-finite coordinates are skipped.
-__global__ void __launch_bounds__(256)
-k_bbox(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, CloudTables t,
-       uint32_t* __restrict__ bbox) {
-  __shared__ float s_red[6][8];
-  const ChunkRange r = chunk_range(t.chunk_base, t.point_off, t.n_clouds, blockIdx.x);
-  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  const uint64_t f0 = (uint64_t)r.begin * 3, f1 = (uint64_t)r.end * 3;
-  // float f >= f0 of the array is component (f - f0) % 3 (f0 is a point's first float)
-  auto fold = [&](uint64_t f, float v) {
-    const uint32_t c = (uint32_t)(f - f0) % 3u;
-    const bool ok = isfinite(v);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      mn[a] = (ok && c == (uint32_t)a) ? fminf(mn[a], v) : mn[a];
-      mx[a] = (ok && c == (uint32_t)a) ? fmaxf(mx[a], v) : mx[a];
-    }
-  };
-  if (aligned) {
-    const uint64_t a0 = f0 & ~3ull;                  // first 16-byte word touching the chunk
-    const uint64_t full_end = total_floats & ~3ull;  // words wholly inside the array
-    const uint64_t nw = (f1 - a0 + 3) >> 2;
-    const float4* w4 = reinterpret_cast<const float4*>(xyz + a0);
-    for (uint64_t w = threadIdx.x; w < nw; w += blockDim.x) {
-      const uint64_t f = a0 + 4 * w;
-      if (f >= f0 && f + 4 <= f1 && f + 4 <= full_end) {
-        const float4 v = __ldg(w4 + w);
-        fold(f, v.x); fold(f + 1, v.y); fold(f + 2, v.z); fold(f + 3, v.w);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if (f + i >= f0 && f + i < f1) fold(f + i, __ldg(xyz + f + i));
-      }
-    }
-  } else {
-    for (uint64_t f = f0 + threadIdx.x; f < f1; f += blockDim.x) fold(f, __ldg(xyz + f));
-  }
+// Each block streams one contiguous range of point chunks straight from HBM: the AoS
+// float3 input is read as 16-byte words (edge words of a chunk and an unaligned input fall
+// back to scalars), and float f of a chunk starting at float f0 is component (f - f0) % 3 of
+// its point, so each thread folds the four floats of a word into the components they
+// belong to -- no staging through shared memory. Per-thread extrema are reduced over the
+// block and merged with one atomic per component only when the range moves on to another
+// cloud, and once at its end. Non-finite coordinates are skipped.
+__device__ __forceinline__ void bbox_flush(float* mn, float* mx, float (*s_red)[8],
+                                           uint32_t cloud, uint32_t n_clouds, uint32_t* bbox) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int a = 0; a < 3; ++a) { mn[a] = warp_min(mn[a]); mx[a] = warp_max(mx[a]); }
@@ -134,10 +102,67 @@ k_bbox(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cloud
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
       v = (a < 3) ? fminf(v, s_red[a][w]) : fmaxf(v, s_red[a][w]);
     if (isfinite(v)) {
-      if (a < 3) atomicMin(&bbox[3 * r.cloud + a], f2o(v));
-      else atomicMax(&bbox[3 * t.n_clouds + 3 * r.cloud + (a - 3)], f2o(v));
+      if (a < 3) atomicMin(&bbox[3 * cloud + a], f2o(v));
+      else atomicMax(&bbox[3 * n_clouds + 3 * cloud + (a - 3)], f2o(v));
     }
   }
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { mn[a] = INFINITY; mx[a] = -INFINITY; }
+}
+
+__global__ void __launch_bounds__(256)
+k_bbox(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, CloudTables t,
+       uint32_t n_chunks, uint32_t* __restrict__ bbox) {
+  __shared__ float s_red[6][8];
+  __shared__ uint32_t s_cloud;
+  const uint32_t per = (n_chunks + gridDim.x - 1) / gridDim.x;
+  const uint32_t c0 = min(n_chunks, blockIdx.x * per), c1 = min(n_chunks, c0 + per);
+  if (c0 >= c1) return;
+  if (threadIdx.x == 0) s_cloud = find_cloud(t.chunk_base, t.n_clouds, c0);
+  __syncthreads();
+  uint32_t cloud = s_cloud;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t chunk = c0; chunk < c1; ++chunk) {
+    while (chunk >= __ldg(t.chunk_base + cloud + 1)) {   // the range moved to the next cloud
+      bbox_flush(mn, mx, s_red, cloud, t.n_clouds, bbox);
+      ++cloud;
+    }
+    const uint32_t pb = __ldg(t.point_off + cloud), pe = __ldg(t.point_off + cloud + 1);
+    const uint32_t begin = pb + (chunk - __ldg(t.chunk_base + cloud)) * (uint32_t)kChunk;
+    const uint32_t end = min(begin + (uint32_t)kChunk, pe);
+    const uint64_t f0 = (uint64_t)begin * 3, f1 = (uint64_t)end * 3;
+    // float f >= f0 of the array is component (f - f0) % 3 (f0 is a point's first float)
+    auto fold = [&](uint64_t f, float v) {
+      const uint32_t c = (uint32_t)(f - f0) % 3u;
+      const bool ok = isfinite(v);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = (ok && c == (uint32_t)a) ? fminf(mn[a], v) : mn[a];
+        mx[a] = (ok && c == (uint32_t)a) ? fmaxf(mx[a], v) : mx[a];
+      }
+    };
+    if (aligned) {
+      const uint64_t a0 = f0 & ~3ull;                  // first 16-byte word touching the chunk
+      const uint64_t full_end = total_floats & ~3ull;  // words wholly inside the array
+      const uint64_t nw = (f1 - a0 + 3) >> 2;
+      const float4* w4 = reinterpret_cast<const float4*>(xyz + a0);
+      for (uint64_t w = threadIdx.x; w < nw; w += blockDim.x) {
+        const uint64_t f = a0 + 4 * w;
+        if (f >= f0 && f + 4 <= f1 && f + 4 <= full_end) {
+          const float4 v = __ldg(w4 + w);
+          fold(f, v.x); fold(f + 1, v.y); fold(f + 2, v.z); fold(f + 3, v.w);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (f + i >= f0 && f + i < f1) fold(f + i, __ldg(xyz + f + i));
+        }
+      }
+    } else {
+      for (uint64_t f = f0 + threadIdx.x; f < f1; f += blockDim.x) fold(f, __ldg(xyz + f));
+    }
+  }
+  bbox_flush(mn, mx, s_red, cloud, t.n_clouds, bbox);
 }
 
 // One block: per-cloud grid geometry and the global cell offsets (block-wide scan over
@@ -368,12 +393,13 @@ cudaError_t launch_single_tables(uint32_t* tab, uint32_t n_points, uint32_t n_qu
 }
 
 cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
-                        uint32_t n_chunks, uint32_t* bbox, cudaStream_t s) {
+                        uint32_t n_chunks, uint32_t* bbox, int n_sms, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(bbox, 0xff, 3ull * t.n_clouds * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(bbox + 3ull * t.n_clouds, 0, 3ull * t.n_clouds * 4, s);
   if (e != cudaSuccess) return e;
   if (n_chunks == 0) return cudaSuccess;
-  k_bbox<<<n_chunks, 256, 0, s>>>(xyz, 3 * n_points, aligned, t, bbox);
+  const unsigned blocks = (unsigned)min((uint64_t)n_chunks, (uint64_t)n_sms * 8);
+  k_bbox<<<blocks, 256, 0, s>>>(xyz, 3 * n_points, aligned, t, n_chunks, bbox);
   return cudaGetLastError();
 }
 

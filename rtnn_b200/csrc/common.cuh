@@ -138,32 +138,34 @@ __device__ __forceinline__ uint64_t morton3_64(uint32_t x, uint32_t y, uint32_t 
 // and the transposed words interleave bit by bit, the first word most significant.
 // Consecutive indices are face-adjacent cells, so a run of consecutive queries stays
 // compact where the Morton order jumps.
+// Every step is a select, not a branch (the lanes of a warp never diverge), and the final
+// Gray-code correction t = XOR of (Q - 1) over the set bits Q > 1 of X2 is a prefix XOR
+// of X2's bits taken from the top, shifted down by one. For x, y, z < 2^b this gives the
+// same index as the step-by-step form of the published method (checked on 3.2 M inputs,
+// b = 1..16).
 __device__ __forceinline__ uint64_t hilbert3_64(uint32_t x, uint32_t y, uint32_t z, uint32_t b) {
   uint32_t X0 = x, X1 = y, X2 = z;
-  const uint32_t M = 1u << (b - 1);
-  for (uint32_t Q = M; Q > 1; Q >>= 1) {
-    const uint32_t P = Q - 1;
-    if (X0 & Q) X0 ^= P;
-    if (X1 & Q) {
-      X0 ^= P;
-    } else {
-      const uint32_t t = (X0 ^ X1) & P;
-      X0 ^= t;
-      X1 ^= t;
-    }
-    if (X2 & Q) {
-      X0 ^= P;
-    } else {
-      const uint32_t t = (X0 ^ X2) & P;
-      X0 ^= t;
-      X2 ^= t;
-    }
+  for (int s = (int)b - 1; s > 0; --s) {
+    const uint32_t Q = 1u << s, P = Q - 1;
+    X0 ^= (X0 & Q) ? P : 0u;
+    const uint32_t t1 = (X0 ^ X1) & P;
+    const bool b1 = (X1 & Q) != 0;
+    X0 ^= b1 ? P : t1;
+    X1 ^= b1 ? 0u : t1;
+    const uint32_t t2 = (X0 ^ X2) & P;
+    const bool b2 = (X2 & Q) != 0;
+    X0 ^= b2 ? P : t2;
+    X2 ^= b2 ? 0u : t2;
   }
   X1 ^= X0;
   X2 ^= X1;
-  uint32_t t = 0;
-  for (uint32_t Q = M; Q > 1; Q >>= 1)
-    if (X2 & Q) t ^= Q - 1;
+  uint32_t v = X2 & ~1u;
+  v ^= v >> 1;
+  v ^= v >> 2;
+  v ^= v >> 4;
+  v ^= v >> 8;
+  v ^= v >> 16;
+  const uint32_t t = v >> 1;
   return morton3_64(X2 ^ t, X1 ^ t, X0 ^ t);
 }
 

@@ -74,7 +74,7 @@ cudaError_t radix_sort_pairs(bool key64, void* keys0, uint32_t* vals0, void* key
 cudaError_t launch_single_tables(uint32_t* tab, uint32_t n_points, uint32_t n_queries,
                                  cudaStream_t s);
 cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const CloudTables& t,
-                        uint32_t n_chunks, uint32_t* bbox, cudaStream_t s);
+                        uint32_t n_chunks, uint32_t* bbox, int n_sms, cudaStream_t s);
 cudaError_t launch_grid_plan(const CloudTables& t, const uint32_t* bbox, float radius,
                              float cell_ratio, float min_cell_ratio, float points_per_cell,
                              float cell_budget, uint32_t order_bits, uint64_t cell_capacity,

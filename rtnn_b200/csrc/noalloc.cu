@@ -235,7 +235,7 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
   bool in1 = false;
   cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(Counters), s);
   if (e == cudaSuccess) e = launch_single_tables(tables, (uint32_t)N, (uint32_t)Q, s);
-  if (e == cudaSuccess) e = launch_bbox(d_points, N, ap, t, n_chunks, bbox, s);
+  if (e == cudaSuccess) e = launch_bbox(d_points, N, ap, t, n_chunks, bbox, n_sms, s);
   if (e == cudaSuccess)
     e = launch_grid_plan(t, bbox, radius, 0.5f, 0.0625f, 0.f, cell_budget, mb, cap, grids, ctr, s);
   if (e == cudaSuccess) e = launch_zero_cells(cells, ctr, n_sms, s);

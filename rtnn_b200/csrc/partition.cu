@@ -167,8 +167,20 @@ k_widths(WidthArgs a) {
   // same cell rows); only the points placed in cells are there, the rest keep no width
   // (that happens only when the grid plan failed, which the call reports as an error)
   const uint32_t n_items = a.spts ? min(a.n_queries, __ldg(a.cells + total_cells)) : a.n_queries;
-  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items;
-       it += gridDim.x * blockDim.x) {
+  // each block walks one contiguous range of items, so a thread's items only move forward
+  // through the clouds: the cloud of the block's first item is looked up once, and each
+  // item then advances the thread's cloud while it lies past that cloud's end (the clouds
+  // are contiguous both in query order and in the cell-sorted point order)
+  const uint32_t* off = a.spts ? a.t.point_off : a.t.query_off;
+  const uint32_t per_block = (n_items + gridDim.x - 1) / gridDim.x;
+  const uint32_t b0 = min(n_items, blockIdx.x * per_block);
+  const uint32_t b1 = min(n_items, b0 + per_block);
+  __shared__ uint32_t s_cloud0;
+  if (threadIdx.x == 0) s_cloud0 = b0 < b1 ? find_cloud(off, a.t.n_clouds, b0) : 0u;
+  __syncthreads();
+  uint32_t cloud = s_cloud0;
+  for (uint32_t it = b0 + threadIdx.x; it < b1; it += blockDim.x) {
+    while (cloud + 1 < a.t.n_clouds && it >= __ldg(off + cloud + 1)) ++cloud;
     uint32_t i = it;
     float qx, qy, qz;
     if (a.spts) {
@@ -179,7 +191,6 @@ k_widths(WidthArgs a) {
     } else {
       qx = __ldg(a.xyz + 3ull * i); qy = __ldg(a.xyz + 3ull * i + 1); qz = __ldg(a.xyz + 3ull * i + 2);
     }
-    const uint32_t cloud = find_cloud(a.t.query_off, a.t.n_clouds, i);
     const CloudGrid g = a.grids[cloud];
     if ((uint64_t)g.cell_base + g.n_cells > (uint64_t)total_cells) {  // overran: full radius
       a.qwidth[i] = a.radius;
