@@ -48,8 +48,8 @@ __device__ __forceinline__ MlpView mlp_view(const float* P) {
 // layer uses packed FP32x2 FMAs (sm_100a): two hidden units per instruction, each element
 // rounded like fmaf, accumulated over the inputs in order, so the result is the bits of the
 // plain one-unit-at-a-time loop. W2p holds W2 with the rows of units 2m and 2m + 1
-// interleaved ({W2[2m][i], W2[2m+1][i]} at W2p[m * 2 * kHidden + 2 i]), one 8-byte load per
-// pair.
+// interleaved ({W2[2m][i], W2[2m+1][i]} at W2p[m * 2 * kHidden + 2 i]; 16-byte aligned),
+// one 16-byte load per two inputs.
 __device__ __forceinline__ uint64_t f2pack(float lo, float hi) {
   uint64_t r;
   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
@@ -94,9 +94,14 @@ __device__ __forceinline__ float mlp_forward_norm_x2(const MlpView& m, const flo
 #pragma unroll 1
   for (int j = 0; j < kHidden; j += 2) {
     uint64_t acc = f2pack(m.b2[j], m.b2[j + 1]);
-    const uint64_t* w = reinterpret_cast<const uint64_t*>(W2p + j * kHidden);
+    // two inputs per 16-byte load: {W2[j][i], W2[j+1][i], W2[j][i+1], W2[j+1][i+1]}
+    const float4* w = reinterpret_cast<const float4*>(W2p + j * kHidden);
 #pragma unroll
-    for (int i = 0; i < kHidden; ++i) acc = fma2(w[i], f2pack(h1[i], h1[i]), acc);
+    for (int i = 0; i < kHidden; i += 2) {
+      const float4 ww = w[i >> 1];
+      acc = fma2(f2pack(ww.x, ww.y), f2pack(h1[i], h1[i]), acc);
+      acc = fma2(f2pack(ww.z, ww.w), f2pack(h1[i + 1], h1[i + 1]), acc);
+    }
     float s0, s1;
     f2unpack(acc, s0, s1);
     o = fmaf(m.W3[j], fmaxf(s0, 0.f), o);
@@ -159,7 +164,7 @@ __device__ __forceinline__ float wmax_f(float v) {
 __global__ void __launch_bounds__(256)
 k_widths(WidthArgs a) {
   __shared__ float s_model[kModelParams];
-  __shared__ __align__(8) float s_w2p[kHidden * kHidden];   // W2, unit pairs interleaved
+  __shared__ __align__(16) float s_w2p[kHidden * kHidden];   // W2, unit pairs interleaved
   if (a.model) load_model_smem(a.model, s_model, s_w2p);
   const MlpView mv = mlp_view(s_model);
   const uint32_t total_cells = a.total_cells ? *a.total_cells : 0u;
@@ -393,7 +398,7 @@ __global__ void __launch_bounds__(256)
 k_mlp_forward(const float* __restrict__ P, const float* __restrict__ feats, uint32_t n,
               float* __restrict__ y) {
   __shared__ float s_p[kModelParams];
-  __shared__ __align__(8) float s_w2p[kHidden * kHidden];
+  __shared__ __align__(16) float s_w2p[kHidden * kHidden];
   load_model_smem(P, s_p, s_w2p);
   const MlpView m = mlp_view(s_p);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

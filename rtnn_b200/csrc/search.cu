@@ -140,6 +140,25 @@ __device__ __forceinline__ float4 stage_get(const float* st, uint32_t slot) {
   return make_float4(b[0], b[2], b[4], b[6]);
 }
 
+// Splits a row number rq of a box nx rows wide into (rq % n, rq / n) for an n fixed over a
+// walk: a float estimate of the quotient corrected by one step, exact while rq / n < 2^22
+// (rows of a box; `exact` false only for boxes of more than 2^22 rows, which divide).
+struct RowSplit {
+  uint32_t n;
+  float inv;
+  bool exact;
+  __device__ __forceinline__ RowSplit(uint32_t n_, uint32_t total) : n(n_), inv(1.0f / (float)n_),
+                                                                     exact(total < (1u << 22)) {}
+  __device__ __forceinline__ void split(uint32_t rq, uint32_t& rem, uint32_t& quo) const {
+    if (!exact) { quo = rq / n; rem = rq - quo * n; return; }
+    uint32_t q = __float2uint_rz((float)rq * inv);
+    int r = (int)rq - (int)(q * n);
+    if (r < 0) { --q; r += (int)n; } else if (r >= (int)n) { ++q; r -= (int)n; }
+    quo = q;
+    rem = (uint32_t)r;
+  }
+};
+
 constexpr int kCheck = 4;          // candidates tested between two buffer-full votes
 constexpr uint32_t kFixedPending = 16;   // appended-hit slots of the compiled-K searches
 constexpr uint32_t kQueryCap = 128;   // k_search_q hit buffer per warp (k <= 64)
@@ -558,17 +577,26 @@ k_search(SearchArgs a) {
         tested += (sum + 31) / 32;
       }
 
+      // rows in a scattered order (stride permutation: kRowStride is a prime above any row
+      // count, so i -> i * kRowStride mod nrows is a bijection of [0, nrows)): a lane's hits
+      // are spread over the walk instead of arriving in one burst, which keeps the lanes'
+      // appended counts level and the merges short. With s = kRowStride mod nrows, row
+      // number ri + 32 is row number ri plus 32 s (mod nrows): three 64-bit remainders per
+      // group, then one add and one compare per batch of 32 rows.
+      uint32_t rq = 0, step32 = 0;
+      if (nrows > 0) {
+        const uint64_t sn = kRowStride % (uint64_t)nrows;
+        rq = (uint32_t)(((uint64_t)lane * sn) % (uint64_t)nrows);
+        step32 = (uint32_t)((32ull * sn) % (uint64_t)nrows);
+      }
+      const RowSplit split(ny > 0 ? (uint32_t)ny : 1u, (uint32_t)nrows);
       for (int rb = 0; rb < (lane_walk ? 0 : nrows); rb += 32) {
         uint32_t rs = 0, re = 0;
         const int ri = rb + lane;
         if (ri < nrows) {
-          // rows in a scattered order (stride permutation: kRowStride is a prime above any
-          // row count, so i -> i * kRowStride mod nrows is a bijection of [0, nrows); the
-          // product stays below 2^63): a lane's hits are
-          // spread over the walk instead of arriving in one burst, which keeps the lanes'
-          // appended counts level and the merges short
-          const int rq = (int)(((uint64_t)ri * kRowStride) % (uint64_t)nrows);
-          const int cy = ly + rq % ny, cz = lz + rq / ny;
+          uint32_t ry, rz;
+          split.split(rq, ry, rz);
+          const int cy = ly + (int)ry, cz = lz + (int)rz;
           int xl, xh;
           if (clip.row(cy, cz, lx, hx, xl, xh)) {
             const uint32_t rowc =
@@ -577,6 +605,8 @@ k_search(SearchArgs a) {
             re = __ldg(a.cells + rowc + xh + 1);
           }
         }
+        rq += step32;
+        if (rq >= (uint32_t)nrows) rq -= (uint32_t)nrows;
         // the (up to) 32 rows as one sequence of candidates: an inclusive scan of the row
         // lengths; candidate t belongs to the row whose scanned end is the first above t
         const uint32_t len = re - rs;
@@ -877,12 +907,15 @@ k_search_q(SearchArgs a) {
       hit_window(true, limj, INFINITY, KNN, wlo, wspan);
       uint32_t nb = 0;       // hits in the buffer (warp-uniform)
       bool stop = false;     // any_k: k hits found
+      const RowSplit split(ny > 0 ? (uint32_t)ny : 1u, (uint32_t)nrows);
       for (int rb = 0; rb < nrows && !stop; rb += 32) {
         uint32_t rs = 0, re = 0;
         const int ri = rb + lane;
         int xl, xh;
-        if (ri < nrows && clip.row(ly + ri % ny, lz + ri / ny, lx, hx, xl, xh)) {
-          const int cy = ly + ri % ny, cz = lz + ri / ny;
+        uint32_t ry = 0, rz = 0;
+        if (ri < nrows) split.split((uint32_t)ri, ry, rz);
+        const int cy = ly + (int)ry, cz = lz + (int)rz;
+        if (ri < nrows && clip.row(cy, cz, lx, hx, xl, xh)) {
           const uint32_t rowc = g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
           rs = __ldg(a.cells + rowc + xl);
           re = __ldg(a.cells + rowc + xh + 1);
