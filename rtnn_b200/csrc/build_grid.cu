@@ -147,15 +147,29 @@ k_bbox(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cloud
       const uint64_t full_end = total_floats & ~3ull;  // words wholly inside the array
       const uint64_t nw = (f1 - a0 + 3) >> 2;
       const float4* w4 = reinterpret_cast<const float4*>(xyz + a0);
-      for (uint64_t w = threadIdx.x; w < nw; w += blockDim.x) {
-        const uint64_t f = a0 + 4 * w;
-        if (f >= f0 && f + 4 <= f1 && f + 4 <= full_end) {
-          const float4 v = __ldg(w4 + w);
-          fold(f, v.x); fold(f + 1, v.y); fold(f + 2, v.z); fold(f + 3, v.w);
-        } else {
+      // four words per thread in flight: the loads of a round are issued before any fold
+      for (uint64_t w0 = threadIdx.x; w0 < nw; w0 += 4ull * blockDim.x) {
+        float4 v[4];
+        bool whole[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
-            if (f + i >= f0 && f + i < f1) fold(f + i, __ldg(xyz + f + i));
+        for (int u = 0; u < 4; ++u) {
+          const uint64_t w = w0 + (uint64_t)u * blockDim.x;
+          const uint64_t f = a0 + 4 * w;
+          whole[u] = w < nw && f >= f0 && f + 4 <= f1 && f + 4 <= full_end;
+          v[u] = whole[u] ? __ldg(w4 + w) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const uint64_t w = w0 + (uint64_t)u * blockDim.x;
+          if (w >= nw) continue;
+          const uint64_t f = a0 + 4 * w;
+          if (whole[u]) {
+            fold(f, v[u].x); fold(f + 1, v[u].y); fold(f + 2, v[u].z); fold(f + 3, v[u].w);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (f + i >= f0 && f + i < f1) fold(f + i, __ldg(xyz + f + i));
+          }
         }
       }
     } else {

@@ -346,7 +346,7 @@ __device__ __forceinline__ float wmax(float v) {
 // query, or a grid that overran the cell array, keeps the full radius.
 __device__ __forceinline__ float learned_tile_width(const SearchArgs& a, uint32_t cloud,
                                                    const float4& q, bool valid,
-                                                   uint32_t total_cells) {
+                                                   uint32_t total_cells, float* scratch) {
   if (!__any_sync(0xffffffffu, valid)) return a.radius;
   const float bx0 = wmin(valid ? q.x : INFINITY), bx1 = wmax(valid ? q.x : -INFINITY);
   const float by0 = wmin(valid ? q.y : INFINITY), by1 = wmax(valid ? q.y : -INFINITY);
@@ -354,7 +354,7 @@ __device__ __forceinline__ float learned_tile_width(const SearchArgs& a, uint32_
   const CloudGrid g = a.grids[cloud];
   if ((uint64_t)g.cell_base + g.n_cells > (uint64_t)total_cells) return a.radius;
   return tile_width(g, a.cells, a.model, a.margin, bx0, bx1, by0, by1, bz0, bz1, a.k + 1,
-                    a.radius);
+                    a.radius, scratch);
 }
 
 // KC > 0: the search for K == KC compiled in (the reference compiles its K in,
@@ -410,7 +410,8 @@ k_search(SearchArgs a) {
     const bool in_range = valid;
     float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
     valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
-    if (main_pass && a.model) wq = learned_tile_width(a, cloud, q, valid, total_cells);
+    // the stage is free between tiles: it lends the width model its 32 floats
+    if (main_pass && a.model) wq = learned_tile_width(a, cloud, q, valid, total_cells, stage);
     if (a.width_out && main_pass && in_range) a.width_out[__float_as_uint(q.w)] = wq;
     float w = a.radius, lim = a.r2;
     if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
@@ -861,7 +862,9 @@ k_search_q(SearchArgs a) {
     const bool in_range = valid;
     const float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
     valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
-    if (main_pass && a.model) wq = learned_tile_width(a, cloud, q, valid, total_cells);
+    // the hit buffer is free between tiles: it lends the width model its 32 floats
+    if (main_pass && a.model)
+      wq = learned_tile_width(a, cloud, q, valid, total_cells, reinterpret_cast<float*>(buf));
     if (a.width_out && main_pass && in_range) a.width_out[__float_as_uint(q.w)] = wq;
     float w = a.radius, lim = a.r2;
     if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }

@@ -81,9 +81,14 @@ __device__ __forceinline__ void tile_features(const CloudGrid& g, const uint32_t
 // The model's prediction (denormalised: log(K-th distance / cell)) for one feature vector.
 // Parameter layout (floats): in_mean[6] in_std[6] out_mean out_std | W1[32][6] b1[32]
 // W2[32][32] b2[32] W3[32] b3, P at least 8-byte aligned (a device allocation is). Lane j
-// computes hidden unit j of both layers; the second layer gathers the first layer's units
-// with shuffles, the output is a warp sum.
-__device__ __forceinline__ float tile_mlp(const float* __restrict__ P, const float* feat) {
+// computes hidden unit j of both layers; the first layer's units reach every lane through
+// `scratch` (32 floats of this warp's shared memory, 16-byte aligned), read back as eight
+// broadcast 16-byte loads, and the second layer sums in four independent chains, so the
+// evaluation is a few short dependency chains instead of 32 shuffles in a row; the output is
+// a warp sum. (The sums run in another order than the inference kernel's: the two agree to
+// FP32 rounding, which only moves a search width, never a result.)
+__device__ __forceinline__ float tile_mlp(const float* __restrict__ P, const float* feat,
+                                          float* scratch) {
   constexpr int F = kTileFeat, H = kTileHidden;
   const int j = threadIdx.x & 31;
   const float* W1 = P + 2 * F + 2;
@@ -93,34 +98,43 @@ __device__ __forceinline__ float tile_mlp(const float* __restrict__ P, const flo
   const float* W3 = b2 + H;
   float xn[F];
 #pragma unroll
-  for (int f = 0; f < F; ++f) xn[f] = (feat[f] - __ldg(P + f)) / __ldg(P + F + f);
+  for (int f = 0; f < F; ++f) xn[f] = __fdividef(feat[f] - __ldg(P + f), __ldg(P + F + f));
   float h1 = __ldg(b1 + j);
 #pragma unroll
   for (int f = 0; f < F; ++f) h1 = fmaf(__ldg(W1 + j * F + f), xn[f], h1);
-  h1 = fmaxf(h1, 0.f);
-  float h2 = __ldg(b2 + j);
+  __syncwarp();
+  scratch[j] = fmaxf(h1, 0.f);
+  __syncwarp();
   // W2 starts 238 floats into P: 8-byte aligned (P itself is 256-byte aligned), not 16
   const float2* w2 = reinterpret_cast<const float2*>(W2 + j * H);
+  const float4* hv = reinterpret_cast<const float4*>(scratch);
+  float acc[4] = {__ldg(b2 + j), 0.f, 0.f, 0.f};
 #pragma unroll
-  for (int i2 = 0; i2 < H / 2; ++i2) {
-    const float2 w = __ldg(w2 + i2);
-    h2 = fmaf(w.x, __shfl_sync(0xffffffffu, h1, 2 * i2), h2);
-    h2 = fmaf(w.y, __shfl_sync(0xffffffffu, h1, 2 * i2 + 1), h2);
+  for (int i4 = 0; i4 < H / 4; ++i4) {
+    const float4 h = hv[i4];
+    const float2 wa = __ldg(w2 + 2 * i4), wb = __ldg(w2 + 2 * i4 + 1);
+    acc[0] = fmaf(wa.x, h.x, acc[0]);
+    acc[1] = fmaf(wa.y, h.y, acc[1]);
+    acc[2] = fmaf(wb.x, h.z, acc[2]);
+    acc[3] = fmaf(wb.y, h.w, acc[3]);
   }
-  h2 = fmaxf(h2, 0.f);
+  __syncwarp();
+  const float h2 = fmaxf((acc[0] + acc[1]) + (acc[2] + acc[3]), 0.f);
   const float o = warp_sum_f(__ldg(W3 + j) * h2) + __ldg(W3 + H);
   return fmaf(o, __ldg(P + 2 * F + 1), __ldg(P + 2 * F));
 }
 
 // Search width of a tile from its features: margin * cell * exp(prediction), at most r.
+// scratch: 32 floats of the warp's shared memory (16-byte aligned) for the MLP.
 __device__ __forceinline__ float tile_width(const CloudGrid& g, const uint32_t* __restrict__ cells,
                                             const float* __restrict__ model, float margin,
                                             float bx0, float bx1, float by0, float by1, float bz0,
-                                            float bz1, uint32_t need, float radius) {
+                                            float bz1, uint32_t need, float radius,
+                                            float* scratch) {
   float feat[kTileFeat];
   tile_features(g, cells, bx0, bx1, by0, by1, bz0, bz1, need, radius, feat);
-  const float y = tile_mlp(model, feat);
-  const float w = margin * g.cell * expf(fminf(y, 30.f));
+  const float y = tile_mlp(model, feat, scratch);
+  const float w = margin * g.cell * __expf(fminf(y, 30.f));
   return w < radius ? w : radius;
 }
 
