@@ -200,8 +200,12 @@ typedef struct rtnn_tuning {
                                  warp per query -- each query walks only its own candidate
                                  box and keeps its hits with warp-wide sorts (narrow widths);
                                  2: tiles for the first pass, one warp per query for the
-                                 escalation passes (scattered short queries). K <= 64 for
-                                 the per-query kernel; larger K always use the tiles */
+                                 escalation passes (scattered short queries); 3: the lane
+                                 walk for the first pass -- each lane of a 32-query tile
+                                 walks only the cells of its own query's box (dense clouds,
+                                 narrow per-query widths) -- and one warp per query for the
+                                 escalation passes; 4: the lane walk in every pass. K <= 64
+                                 for the per-query kernel; larger K use the tiles there */
   float buckets_per_halving;  /* partitioned search: density buckets (sort-key levels) per
                                  halving of the search width (0..8; 0: all narrowed widths
                                  in one bucket). Fewer buckets keep tiles spatially tighter,
@@ -209,9 +213,13 @@ typedef struct rtnn_tuning {
   uint32_t width_model;       /* RTNN_FLAG_LEARNED: 0: a width per query from the model before
                                  the query sort, queries bucketed by width (one more pass,
                                  tight boxes); 1: a width per 32-query tile, evaluated by the
-                                 search kernel itself (no extra pass, one box per tile). The
-                                 model is trained for one kind (rtnn_collect_training follows
-                                 this setting) */
+                                 search kernel itself (no extra pass, one box per tile); 2:
+                                 the widths are off -- a learned search takes every query at
+                                 the full radius, exactly as the plain search does (the
+                                 autotuner's choice where narrowed widths cannot pay: most
+                                 K-th distances at r, or a grid already tight around them).
+                                 The model is trained for one kind (rtnn_collect_training
+                                 follows this setting; 2 collects per-query samples) */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

@@ -35,7 +35,7 @@ SEARCH_KNOBS = [
     ("lane_walk_ratio", [0.0, 0.5, 1.0, 2.0]),
     ("gap_ratio", [0.0, 1.0, 2.0, 4.0]),
     ("pending_slots", [8, 16, 32, 64]),
-    ("query_warps", [0, 1, 2]),
+    ("query_warps", [0, 1, 2, 3]),
 ]
 GRID_KNOBS = CELL_KNOBS + SEARCH_KNOBS
 # whole cell-size regimes tried as starting points: one knob at a time would not move from
@@ -159,6 +159,7 @@ def autotune(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radi
 
 
 WIDTH_MODELS = [0, 1]   # rtnn_tuning.width_model: per query before the sort, per tile in the search
+OFF = 2                 # rtnn_tuning.width_model: learned widths switched off (full radius)
 MARGINS = [0.8, 0.9, 1.0, 1.1, 1.25]
 
 
@@ -170,7 +171,10 @@ def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="kn
     model is trained at that setting (`train(ctx)` collects training data and trains; what
     it returns is handed back for the chosen setting) and the width margin is tuned; the
     fastest setting keeps its model, then the search and learned knobs, which leave the
-    grid alone, are tuned by descent. Returns (tuning, train's result for the chosen one)."""
+    grid alone, are tuned by descent. Last, that setting is timed against the widths
+    switched off (width_model 2, the starting tuning: the plain search's) and the faster is
+    kept. Returns (tuning, train's result for the chosen setting plus "widths": "on" or
+    "off" and both times)."""
     import torch
     offsets = np.asarray(offsets, dtype=np.uint64)
     nq = int(offsets[-1]) if queries is None else int(np.asarray(qoffsets)[-1])
@@ -194,6 +198,21 @@ def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="kn
     ctx.set_model(model)
     tun = autotune(ctx, points, offsets, queries, qoffsets, knobs=SEARCH_KNOBS + LEARNED_KNOBS,
                    use_cache=False, log=log, **kw)
+    ms_on = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
+    # the widths switched off (width_model 2: every query at the full radius, the starting
+    # tuning's grid and kernels) where narrowing cannot pay -- most K-th distances at r, or
+    # a grid whose cells already fit the balls -- so the learned search never loses to the
+    # plain one; the model stays loaded
+    off = {**start, "width_model": OFF}
+    ctx.set_tuning(**off)
+    ms_off = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
+    if log:
+        log(f"autotune learned widths on: {ms_on:.3f} ms, off: {ms_off:.3f} ms")
+    if ms_off < ms_on:
+        info = {**(info or {}), "widths": "off", "ms_on": ms_on, "ms_off": ms_off}
+        return off, info
+    ctx.set_tuning(**tun)
+    info = {**(info or {}), "widths": "on", "ms_on": ms_on, "ms_off": ms_off}
     return tun, info
 
 

@@ -260,15 +260,15 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
   return RTNN_OK;
 }
 
+// learned widths, unless the tuning switched them off (width_model 2: the width model
+// cannot pay on this workload, every query is searched at the full radius)
+bool learned(const Params& p) { return (p.flags & RTNN_FLAG_LEARNED) != 0 && p.width_model != 2; }
 // narrowed widths with escalation passes: the analytic partition or the learned widths
-bool partitioned(const Params& p) { return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0; }
-bool learned(const Params& p) { return (p.flags & RTNN_FLAG_LEARNED) != 0; }
+bool partitioned(const Params& p) { return (p.flags & RTNN_FLAG_PARTITION) != 0 || learned(p); }
 // learned widths per 32-query tile, evaluated by the search kernel itself
 bool tile_widths(const Params& p) { return learned(p) && p.width_model == 1; }
 // a width per query before the sort: the analytic partition, or the per-query model
-bool per_query_widths(const Params& p) {
-  return (p.flags & (RTNN_FLAG_PARTITION | RTNN_FLAG_LEARNED)) != 0 && !tile_widths(p);
-}
+bool per_query_widths(const Params& p) { return partitioned(p) && !tile_widths(p); }
 uint32_t level_bits_of(const Params& p) { return per_query_widths(p) ? 4u : 0u; }
 uint32_t key_bits_of(const Shapes& sh, const Params& p) { return sh.key_bits + level_bits_of(p); }
 bool key64_of(const Shapes& sh, const Params& p) { return key_bits_of(sh, p) > 32; }
@@ -445,21 +445,27 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   int wpb = 4;
   fit_search_shape(pr.k, tu.pending_slots, (int)tu.warps_per_block, &a.pending, &wpb);
   a.qcap = search_q_cap(pr.k);   // 0: k too large for one warp's hit buffer
-  // kernel per pass: the tile walk, or one warp per query (query_warps 1: every pass;
-  // 2: the escalation passes only, whose short queries are scattered over the clouds)
+  // kernel per pass: the tile walk, the lane walk or one warp per query (query_warps 1:
+  // one warp per query in every pass; 2: tiles for the first pass, one warp per query for
+  // the escalation passes, whose short queries are scattered over the clouds; 3: the lane
+  // walk for the first pass, one warp per query for the escalation passes; 4: the lane
+  // walk in every pass)
   const bool q_main = tu.query_warps == 1 && a.qcap != 0;
-  const bool q_fallback = tu.query_warps != 0 && a.qcap != 0;
+  const bool q_fallback = (tu.query_warps >= 1 && tu.query_warps <= 3) && a.qcap != 0;
+  const bool l_main = tu.query_warps == 3 || tu.query_warps == 4;
+  const bool l_fallback = tu.query_warps == 4;
   const int wpb_q = (int)std::max(1u, std::min(8u, tu.warps_per_block));
-  auto grid_for = [&](bool per_query, int w) {
+  auto grid_for = [&](bool per_query, bool lanes, int w) {
     int bps = per_query ? search_q_blocks_per_sm(knn, pr.k, w)
-                        : search_blocks_per_sm(knn, pr.k, a.pending, w);
+                        : search_blocks_per_sm(knn, pr.k, a.pending, w, lanes);
     if (tu.blocks_per_sm > 0) bps = std::min(bps, (int)tu.blocks_per_sm);
     const uint64_t persistent = (uint64_t)c->n_sms * bps;
     const uint64_t need_blocks = (sh.n_tiles + w - 1) / w;
     return (unsigned)std::max<uint64_t>(1, std::min(persistent, need_blocks));
   };
-  const unsigned blocks_tile = grid_for(false, wpb);
-  const unsigned blocks_q = a.qcap != 0 ? grid_for(true, wpb_q) : 1u;
+  const unsigned blocks_tile = grid_for(false, false, wpb);
+  const unsigned blocks_lane = grid_for(false, true, wpb);
+  const unsigned blocks_q = a.qcap != 0 ? grid_for(true, false, wpb_q) : 1u;
   // pass 0: every query at its partition width; each pass flags its short queries, an
   // order-preserving compaction (scan of the flags) turns them into list p%2 at a wider
   // width (grown by the density each query saw, at most doubled), and escalation pass p
@@ -482,8 +488,9 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
     a.fb_next_w = flagging ? (float*)ws.fbnextw.p : nullptr;
     if (flagging) RTNN_CU(cudaMemsetAsync(flags, 0, (sh.Q + 1) * 4, s), "memset flags");
     const bool per_query = p == 0 ? q_main : q_fallback;
+    const bool lanes = p == 0 ? l_main : l_fallback;
     RTNN_CU(per_query ? launch_search_q(knn, a, blocks_q, wpb_q, s)
-                      : launch_search(knn, a, blocks_tile, wpb, s),
+                      : launch_search(knn, a, lanes ? blocks_lane : blocks_tile, wpb, lanes, s),
             p == 0 ? "search" : "fallback search");
     if (flagging) {
       const uint32_t* n_dev = p > 0 ? &ctr->fb_count[p - 1] : nullptr;
@@ -835,8 +842,8 @@ rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
       !(t->points_per_cell >= 0.f) || t->fallback_passes > kMaxPasses - 2 ||
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f) ||
       !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f) || t->pending_slots < 8 ||
-      t->pending_slots > 256 || t->query_warps > 2 ||
-      !(t->buckets_per_halving >= 0.f && t->buckets_per_halving <= 8.f) || t->width_model > 1)
+      t->pending_slots > 256 || t->query_warps > 4 ||
+      !(t->buckets_per_halving >= 0.f && t->buckets_per_halving <= 8.f) || t->width_model > 2)
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
   return RTNN_OK;
@@ -1092,6 +1099,9 @@ rtnn_status rtnn_query_widths(rtnn_ctx* c, const float* d_points, uint64_t n_poi
   c->err.clear();
   if (d_queries == nullptr) n_queries = n_points;
   flags = (flags & RTNN_FLAG_LEARNED) | RTNN_FLAG_PARTITION | RTNN_FLAG_DEVICE_POINTERS;
+  // learned widths switched off by the tuning: the learned search takes every query at r
+  if ((flags & RTNN_FLAG_LEARNED) && c->tuning.width_model == 2)
+    flags = RTNN_FLAG_LEARNED | RTNN_FLAG_DEVICE_POINTERS;
   rtnn_status st = check_args(c, n_points, n_queries, radius, k, flags);
   if (st != RTNN_OK) return st;
   if (n_points == 0 || n_queries == 0) return RTNN_OK;

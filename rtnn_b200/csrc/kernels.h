@@ -99,9 +99,10 @@ cudaError_t launch_gather_queries(const float* xyz, const uint32_t* order, uint3
 
 // search.cu
 constexpr size_t kSearchSmemLimit = 227 * 1024;   // dynamic shared memory per block
-size_t search_smem_bytes(uint32_t k, uint32_t pending, int warps_per_block);
+// lanes: the lane walk (k_search with LANES), which needs no candidate stage
+size_t search_smem_bytes(uint32_t k, uint32_t pending, int warps_per_block, bool lanes);
 cudaError_t search_prepare(int device);
-int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block);
+int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block, bool lanes);
 // K itself when the searches have an instantiation with K compiled in, else 0
 int search_compiled_k(uint32_t k);
 // appended-hit slots (multiple of 4, 8..256) and warps per block that fit the limit
@@ -112,7 +113,7 @@ int search_q_blocks_per_sm(bool knn, uint32_t k, int warps_per_block);
 cudaError_t launch_search_q(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
                             cudaStream_t s);
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
-                          cudaStream_t s);
+                          bool lanes, cudaStream_t s);
 cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, const uint32_t* n_dev,
                                     const CloudTables& t, const uint32_t* in_pos,
                                     const uint32_t* in_cloud, const float* next_w,

@@ -165,7 +165,7 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
           uint32_t pend = 16;
           int wpb = 4;
           fit_search_shape(kk, 16u, 4, &pend, &wpb);
-          g_bps[dev][knn][kk - 1] = search_blocks_per_sm(knn != 0, kk, pend, wpb);
+          g_bps[dev][knn][kk - 1] = search_blocks_per_sm(knn != 0, kk, pend, wpb, false);
         }
       if (e != cudaSuccess || !ptr) {
         cudaGetLastError();
@@ -270,7 +270,7 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
     fit_search_shape(k, 16u, 4, &a.pending, &wpb);
     const uint64_t blocks = (uint64_t)n_sms * g_bps[dev][knn ? 1 : 0][k - 1];
     const uint64_t need = (n_tiles + wpb - 1) / wpb;
-    e = launch_search(knn, a, (unsigned)(blocks < need ? blocks : need), wpb, s);
+    e = launch_search(knn, a, (unsigned)(blocks < need ? blocks : need), wpb, false, s);
   }
   if (e == cudaSuccess) e = publish_and_wait(dev, ctr, s, &timed_out);
   if (e != cudaSuccess) {

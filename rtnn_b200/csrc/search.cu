@@ -163,6 +163,7 @@ constexpr int kCheck = 4;          // candidates tested between two buffer-full 
 constexpr uint32_t kFixedPending = 16;   // appended-hit slots of the compiled-K searches
 constexpr uint32_t kQueryCap = 128;   // k_search_q hit buffer per warp (k <= 64)
 constexpr int kStage = 64;         // staged candidates per warp (float4)
+constexpr int kLaneRows = 8;       // lane walk: cell rows whose offsets are loaded together
 constexpr uint64_t kRowStride = 4294967311ull;   // prime > 2^32 > any row count of a box
 
 // Cell rows of a candidate box clipped to the points within R of the query box, in cell
@@ -362,15 +363,19 @@ __device__ __forceinline__ float learned_tile_width(const SearchArgs& a, uint32_
 // column length and every heap loop bound are constants; KC == 0: any K and slot count.
 // Small compiled K (short result columns, so shared memory allows more resident warps):
 // registers are capped so that 6 blocks of 4 warps fit an SM.
-template <bool KNN, int KC>
+// LANES: every tile is searched lane by lane (each lane walks the cells of its own query's
+// box, no shared candidate stream and no stage): the walk for dense narrow searches, where
+// a tile's shared box holds many times the points of one query's ball.
+template <bool KNN, int KC, bool LANES>
 __global__ void __launch_bounds__(256, (KC > 0 && KC <= 16) ? 3 : 2)
 k_search(SearchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  float* stage = reinterpret_cast<float*>(smem) + warp * kStage * 4;   // pair layout
   const uint32_t k = KC > 0 ? (uint32_t)KC : a.k;
   const uint32_t slots = k + (KC > 0 ? kFixedPending : a.pending);   // column length per lane
-  uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * kStage * 16) +
+  const size_t stage_bytes = LANES ? 0 : (size_t)kStage * 16;
+  float* stage = reinterpret_cast<float*>(smem + (size_t)warp * stage_bytes);   // pair layout
+  uint64_t* heapw = reinterpret_cast<uint64_t*>(smem + (size_t)wpb * stage_bytes) +
                     (size_t)warp * slots * 32;
   uint64_t* col = heapw + lane;   // this lane's column: col[i * 32]
   const uint32_t lt = lanemask_lt();
@@ -410,8 +415,11 @@ k_search(SearchArgs a) {
     const bool in_range = valid;
     float4 q = valid ? a.sq[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
     valid = valid && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
-    // the stage is free between tiles: it lends the width model its 32 floats
-    if (main_pass && a.model) wq = learned_tile_width(a, cloud, q, valid, total_cells, stage);
+    // the stage (the result columns of the lane walk) is free between tiles: it lends the
+    // width model its 32 floats
+    if (main_pass && a.model)
+      wq = learned_tile_width(a, cloud, q, valid, total_cells,
+                              LANES ? reinterpret_cast<float*>(heapw) : stage);
     if (a.width_out && main_pass && in_range) a.width_out[__float_as_uint(q.w)] = wq;
     float w = a.radius, lim = a.r2;
     if (wq < a.radius) { w = wq; lim = __fmul_rn(wq, wq); }
@@ -428,7 +436,7 @@ k_search(SearchArgs a) {
     const uint32_t prc = __shfl_up_sync(0xffffffffu, cloud, 1);
     const bool prv = __shfl_up_sync(0xffffffffu, valid ? 1u : 0u, 1) != 0u;
     bool run_start = valid && (lane == 0 || !prv || prc != cloud);
-    if (valid && !run_start && a.gap_ratio > 0.f) {
+    if (!LANES && valid && !run_start && a.gap_ratio > 0.f) {
       const float ex = q.x - prx, ey = q.y - pry, ez = q.z - prz;
       run_start = ex * ex + ey * ey + ez * ez > gap * gap;
     }
@@ -524,58 +532,132 @@ k_search(SearchArgs a) {
       // walk per lane: each lane visits only the cells of its own query's box, so it tests
       // a few times K points instead of everything near the whole tile.
       const float spread = fmaxf(fmaxf(bx1 - bx0, by1 - by0), bz1 - bz0);
-      const bool lane_walk = a.lane_walk_ratio > 0.f && spread > a.lane_walk_ratio * R;
+      const bool lane_walk = LANES || (a.lane_walk_ratio > 0.f && spread > a.lane_walk_ratio * R);
 
       if (lane_walk) {
-        const float INF = INFINITY;
-        const float4 far = make_float4(INF, INF, INF, 0.f);
-        int l0 = 0, h0 = -1, l1 = 0, h1 = -1, l2 = 0, h2 = -1;
-        if (act && grid_ok) {
-          const float Rl = __fmul_ru(w, 1.000001f);
-          const float gx0 = cell_coord_f(__fsub_rn(q.x, Rl), g.ox, g.inv_cell);
-          const float gx1 = cell_coord_f(__fadd_rn(q.x, Rl), g.ox, g.inv_cell);
-          const float gy0 = cell_coord_f(__fsub_rn(q.y, Rl), g.oy, g.inv_cell);
-          const float gy1 = cell_coord_f(__fadd_rn(q.y, Rl), g.oy, g.inv_cell);
-          const float gz0 = cell_coord_f(__fsub_rn(q.z, Rl), g.oz, g.inv_cell);
-          const float gz1 = cell_coord_f(__fadd_rn(q.z, Rl), g.oz, g.inv_cell);
-          if (gx0 <= (float)(g.dx - 1) && gx1 >= 0.f && gy0 <= (float)(g.dy - 1) && gy1 >= 0.f &&
-              gz0 <= (float)(g.dz - 1) && gz1 >= 0.f) {
-            l0 = (int)fmaxf(gx0, 0.f); h0 = (int)fminf(gx1, (float)(g.dx - 1));
-            l1 = (int)fmaxf(gy0, 0.f); h1 = (int)fminf(gy1, (float)(g.dy - 1));
-            l2 = (int)fmaxf(gz0, 0.f); h2 = (int)fminf(gz1, (float)(g.dz - 1));
+        if constexpr (LANES) {
+          // This lane's box: its query +- its own width, rows clipped to the ball
+          // (RowClipPoint). Rows are taken kLaneRows at a time: the row ends of a batch are
+          // computed and their 2 x kLaneRows offset loads issued together, then each row's
+          // points are tested four at a time (loads first, past the row's end points at
+          // infinity). All lanes walk their rows in the same relative order (y fastest from
+          // the low corner of the box), so lanes whose queries share a cell row read the same
+          // cache lines at the same step.
+          const float INF = INFINITY;
+          const float4 far = make_float4(INF, INF, INF, 0.f);
+          int l0 = 0, h0 = -1, l1 = 0, h1 = -1, l2 = 0, h2 = -1;
+          const float Rl = act ? __fmul_ru(w, 1.000001f) : 0.f;
+          if (act && grid_ok) {
+            const float gx0 = cell_coord_f(__fsub_rn(q.x, Rl), g.ox, g.inv_cell);
+            const float gx1 = cell_coord_f(__fadd_rn(q.x, Rl), g.ox, g.inv_cell);
+            const float gy0 = cell_coord_f(__fsub_rn(q.y, Rl), g.oy, g.inv_cell);
+            const float gy1 = cell_coord_f(__fadd_rn(q.y, Rl), g.oy, g.inv_cell);
+            const float gz0 = cell_coord_f(__fsub_rn(q.z, Rl), g.oz, g.inv_cell);
+            const float gz1 = cell_coord_f(__fadd_rn(q.z, Rl), g.oz, g.inv_cell);
+            if (gx0 <= (float)(g.dx - 1) && gx1 >= 0.f && gy0 <= (float)(g.dy - 1) && gy1 >= 0.f &&
+                gz0 <= (float)(g.dz - 1) && gz1 >= 0.f) {
+              l0 = (int)fmaxf(gx0, 0.f); h0 = (int)fminf(gx1, (float)(g.dx - 1));
+              l1 = (int)fmaxf(gy0, 0.f); h1 = (int)fminf(gy1, (float)(g.dy - 1));
+              l2 = (int)fmaxf(gz0, 0.f); h2 = (int)fminf(gz1, (float)(g.dz - 1));
+            }
           }
-        }
-        const int nyl = h1 - l1 + 1;
-        const int nrl = (h0 >= l0 && h1 >= l1 && h2 >= l2) ? nyl * (h2 - l2 + 1) : 0;
-        int ri = 0;
-        uint32_t ptr = 0, end = 0, mine = 0;
-        while (true) {
-          while (ptr >= end && ri < nrl) {   // next non-empty row of this lane's box
-            const int cy = l1 + ri % nyl, cz = l2 + ri / nyl;
-            const uint32_t rowc =
-                g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
-            ptr = __ldg(a.cells + rowc + l0);
-            end = __ldg(a.cells + rowc + h0 + 1);
-            ++ri;
-          }
-          if (!__any_sync(0xffffffffu, ptr < end)) break;
-          // four points of this lane's current row; past its end, points at infinity
-          const float4 p0 = ptr < end ? __ldg(a.spts + ptr) : far;
-          const float4 p1 = ptr + 1 < end ? __ldg(a.spts + ptr + 1) : far;
-          const float4 p2 = ptr + 2 < end ? __ldg(a.spts + ptr + 2) : far;
-          const float4 p3 = ptr + 3 < end ? __ldg(a.spts + ptr + 3) : far;
-          const uint32_t took = min(end - ptr, 4u);
-          mine += took;
-          ptr += took;
-          test4(p0, p1, p2, p3);
-          check();
-        }
-        // counters in units of 32 lane-tests, like one staged point of the shared walk
-        uint32_t sum = mine;
+          const int nrl = (h0 >= l0 && h1 >= l1 && h2 >= l2) ? (h1 - l1 + 1) * (h2 - l2 + 1) : 0;
+          const RowClipPoint lclip(g, q.x, q.y, q.z, Rl);
+          int cy = l1, cz = l2;   // the next row of the walk
+          uint32_t mine = 0;
+          constexpr int kRows = kLaneRows;
+          for (int rb = 0; __any_sync(0xffffffffu, rb < nrl); rb += kRows) {
+            uint32_t rs[kRows], re[kRows];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        loaded += sum;
-        tested += (sum + 31) / 32;
+            for (int j = 0; j < kRows; ++j) {
+              rs[j] = 0u;
+              re[j] = 0u;
+              int xl, xh;
+              if (rb + j < nrl && lclip.row(cy, cz, l0, h0, xl, xh)) {
+                const uint32_t rowc =
+                    g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+                rs[j] = __ldg(a.cells + rowc + xl);
+                re[j] = __ldg(a.cells + rowc + xh + 1);
+              }
+              const bool wrap = cy >= h1;
+              cy = wrap ? l1 : cy + 1;
+              cz = wrap ? cz + 1 : cz;
+            }
+#pragma unroll
+            for (int j = 0; j < kRows; ++j) {
+              uint32_t ptr = rs[j];
+              const uint32_t end = re[j];
+              while (__any_sync(0xffffffffu, ptr < end)) {
+                const float4 p0 = ptr < end ? __ldg(a.spts + ptr) : far;
+                const float4 p1 = ptr + 1 < end ? __ldg(a.spts + ptr + 1) : far;
+                const float4 p2 = ptr + 2 < end ? __ldg(a.spts + ptr + 2) : far;
+                const float4 p3 = ptr + 3 < end ? __ldg(a.spts + ptr + 3) : far;
+                const uint32_t took = ptr < end ? min(end - ptr, 4u) : 0u;
+                mine += took;
+                ptr += took;
+                test4(p0, p1, p2, p3);
+                check();
+              }
+            }
+          }
+          // counters in units of 32 lane-tests, like one staged point of the shared walk
+          uint32_t sum = mine;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+          loaded += sum;
+          tested += (sum + 31) / 32;
+        } else {
+          // the tile walk's spread tiles: one row at a time over the lane's box
+          const float INF = INFINITY;
+          const float4 far = make_float4(INF, INF, INF, 0.f);
+          int l0 = 0, h0 = -1, l1 = 0, h1 = -1, l2 = 0, h2 = -1;
+          if (act && grid_ok) {
+            const float Rl = __fmul_ru(w, 1.000001f);
+            const float gx0 = cell_coord_f(__fsub_rn(q.x, Rl), g.ox, g.inv_cell);
+            const float gx1 = cell_coord_f(__fadd_rn(q.x, Rl), g.ox, g.inv_cell);
+            const float gy0 = cell_coord_f(__fsub_rn(q.y, Rl), g.oy, g.inv_cell);
+            const float gy1 = cell_coord_f(__fadd_rn(q.y, Rl), g.oy, g.inv_cell);
+            const float gz0 = cell_coord_f(__fsub_rn(q.z, Rl), g.oz, g.inv_cell);
+            const float gz1 = cell_coord_f(__fadd_rn(q.z, Rl), g.oz, g.inv_cell);
+            if (gx0 <= (float)(g.dx - 1) && gx1 >= 0.f && gy0 <= (float)(g.dy - 1) && gy1 >= 0.f &&
+                gz0 <= (float)(g.dz - 1) && gz1 >= 0.f) {
+              l0 = (int)fmaxf(gx0, 0.f); h0 = (int)fminf(gx1, (float)(g.dx - 1));
+              l1 = (int)fmaxf(gy0, 0.f); h1 = (int)fminf(gy1, (float)(g.dy - 1));
+              l2 = (int)fmaxf(gz0, 0.f); h2 = (int)fminf(gz1, (float)(g.dz - 1));
+            }
+          }
+          const int nyl = h1 - l1 + 1;
+          const int nrl = (h0 >= l0 && h1 >= l1 && h2 >= l2) ? nyl * (h2 - l2 + 1) : 0;
+          int ri = 0;
+          uint32_t ptr = 0, end = 0, mine = 0;
+          while (true) {
+            while (ptr >= end && ri < nrl) {   // next non-empty row of this lane's box
+              const int cy = l1 + ri % nyl, cz = l2 + ri / nyl;
+              const uint32_t rowc =
+                  g.cell_base + ((uint32_t)cz * (uint32_t)g.dy + (uint32_t)cy) * (uint32_t)g.dx;
+              ptr = __ldg(a.cells + rowc + l0);
+              end = __ldg(a.cells + rowc + h0 + 1);
+              ++ri;
+            }
+            if (!__any_sync(0xffffffffu, ptr < end)) break;
+            // four points of this lane's current row; past its end, points at infinity
+            const float4 p0 = ptr < end ? __ldg(a.spts + ptr) : far;
+            const float4 p1 = ptr + 1 < end ? __ldg(a.spts + ptr + 1) : far;
+            const float4 p2 = ptr + 2 < end ? __ldg(a.spts + ptr + 2) : far;
+            const float4 p3 = ptr + 3 < end ? __ldg(a.spts + ptr + 3) : far;
+            const uint32_t took = min(end - ptr, 4u);
+            mine += took;
+            ptr += took;
+            test4(p0, p1, p2, p3);
+            check();
+          }
+          // counters in units of 32 lane-tests, like one staged point of the shared walk
+          uint32_t sum = mine;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+          loaded += sum;
+          tested += (sum + 31) / 32;
+        }
       }
 
       // rows in a scattered order (stride permutation: kRowStride is a prime above any row
@@ -1047,15 +1129,16 @@ cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, cons
   return cudaGetLastError();
 }
 
-size_t search_smem_bytes(uint32_t k, uint32_t pending, int warps_per_block) {
-  return (size_t)warps_per_block * (kStage * 16 + (size_t)(k + pending) * 32 * 8);
+size_t search_smem_bytes(uint32_t k, uint32_t pending, int warps_per_block, bool lanes) {
+  return (size_t)warps_per_block * ((lanes ? 0 : kStage * 16) + (size_t)(k + pending) * 32 * 8);
 }
 
 void fit_search_shape(uint32_t k, uint32_t pending_req, int wpb_req, uint32_t* pending, int* wpb) {
+  // sized for the tile walk (the lane walk needs no stage, so the same shape fits it)
   uint32_t p = std::max(8u, std::min(256u, pending_req)) & ~3u;
-  while (p > 8 && search_smem_bytes(k, p, 1) > kSearchSmemLimit) p -= 4;
+  while (p > 8 && search_smem_bytes(k, p, 1, false) > kSearchSmemLimit) p -= 4;
   int w = std::max(1, std::min(8, wpb_req));
-  while (w > 1 && search_smem_bytes(k, p, w) > kSearchSmemLimit) --w;
+  while (w > 1 && search_smem_bytes(k, p, w, false) > kSearchSmemLimit) --w;
   *pending = p;
   *wpb = w;
 }
@@ -1072,12 +1155,18 @@ int compiled_k(uint32_t k) {
   return 0;
 }
 
-// kernel entry of k_search / k_search_q for (mode, compiled K or 0)
-const void* search_fn(bool knn, int kc) {
-#define RTNN_CASE(K) if (kc == K) return knn ? (const void*)k_search<true, K> : (const void*)k_search<false, K>;
+// kernel entry of k_search (tile or lane walk) / k_search_q for (mode, compiled K or 0)
+template <bool LANES>
+const void* search_fn_walk(bool knn, int kc) {
+#define RTNN_CASE(K)                                                                       \
+  if (kc == K)                                                                             \
+    return knn ? (const void*)k_search<true, K, LANES> : (const void*)k_search<false, K, LANES>;
   RTNN_COMPILED_KS(RTNN_CASE)
 #undef RTNN_CASE
-  return knn ? (const void*)k_search<true, 0> : (const void*)k_search<false, 0>;
+  return knn ? (const void*)k_search<true, 0, LANES> : (const void*)k_search<false, 0, LANES>;
+}
+const void* search_fn(bool knn, int kc, bool lanes) {
+  return lanes ? search_fn_walk<true>(knn, kc) : search_fn_walk<false>(knn, kc);
 }
 const void* search_q_fn(bool knn, int kc) {
 #define RTNN_CASE(K) if (kc == K) return knn ? (const void*)k_search_q<true, K> : (const void*)k_search_q<false, K>;
@@ -1093,25 +1182,26 @@ int search_compiled_k(uint32_t k) { return compiled_k(k); }
 cudaError_t search_prepare(int device) {
   (void)device;
   cudaError_t e = cudaSuccess;
-  for (int knn = 0; knn < 2 && e == cudaSuccess; ++knn) {
-    e = cudaFuncSetAttribute(search_fn(knn, 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
+  for (int v = 0; v < 4 && e == cudaSuccess; ++v) {
+    const bool knn = v & 1, lanes = v >> 1;
+    e = cudaFuncSetAttribute(search_fn(knn, 0, lanes), cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kSearchSmemLimit);
-#define RTNN_CASE(K)                                                                           \
-    if (e == cudaSuccess)                                                                      \
-      e = cudaFuncSetAttribute(search_fn(knn, K), cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                               (int)kSearchSmemLimit);
+#define RTNN_CASE(K)                                                                      \
+    if (e == cudaSuccess)                                                                 \
+      e = cudaFuncSetAttribute(search_fn(knn, K, lanes),                                  \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSearchSmemLimit);
     RTNN_COMPILED_KS(RTNN_CASE)
 #undef RTNN_CASE
   }
   return e;
 }
 
-int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block) {
+int search_blocks_per_sm(bool knn, uint32_t k, uint32_t pending, int warps_per_block, bool lanes) {
   int nb = 0;
-  const size_t smem = search_smem_bytes(k, pending, warps_per_block);
+  const size_t smem = search_smem_bytes(k, pending, warps_per_block, lanes);
   const int threads = warps_per_block * 32;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &nb, search_fn(knn, tile_kc(k, pending)), threads, smem);
+      &nb, search_fn(knn, tile_kc(k, pending), lanes), threads, smem);
   if (e != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }
@@ -1142,11 +1232,11 @@ cudaError_t launch_search_q(bool knn, const SearchArgs& a, unsigned blocks, int 
 }
 
 cudaError_t launch_search(bool knn, const SearchArgs& a, unsigned blocks, int warps_per_block,
-                          cudaStream_t s) {
-  const size_t smem = search_smem_bytes(a.k, a.pending, warps_per_block);
+                          bool lanes, cudaStream_t s) {
+  const size_t smem = search_smem_bytes(a.k, a.pending, warps_per_block, lanes);
   SearchArgs args = a;
   void* params[] = {&args};
-  return cudaLaunchKernel(search_fn(knn, tile_kc(a.k, a.pending)), dim3(blocks),
+  return cudaLaunchKernel(search_fn(knn, tile_kc(a.k, a.pending), lanes), dim3(blocks),
                           dim3(warps_per_block * 32), params, smem, s);
 }
 

@@ -52,9 +52,9 @@ class FakeCtx:
     def set_tuning(self, **kw):
         ok = (0 < kw["cell_ratio"] <= 64 and 0 < kw["min_cell_ratio"] <= kw["cell_ratio"] and
               kw["points_per_cell"] >= 0 and 1 <= kw["warps_per_block"] <= 8 and
-              8 <= kw["pending_slots"] <= 256 and kw["query_warps"] <= 2 and
+              8 <= kw["pending_slots"] <= 256 and kw["query_warps"] <= 4 and
               kw["fallback_passes"] <= 6 and 0 <= kw["buckets_per_halving"] <= 8 and
-              kw["width_model"] <= 1)
+              kw["width_model"] <= 2)
         if not ok:
             self.rejected += 1
             raise rtnn_b200.RtnnError(1, "tuning values out of range")
@@ -149,9 +149,26 @@ def test_learned_keeps_the_model_of_the_winning_preset():
                                     train=train)
     assert trained == [(p["cell_ratio"], kind) for p in at.GRID_PRESETS for kind in (0, 1)]
     assert tun["cell_ratio"] == 0.25 and tun["width_model"] == 1
-    assert info == {"preset": 0.25, "kind": 1}
+    assert {n: info[n] for n in ("preset", "kind", "widths")} == {"preset": 0.25, "kind": 1,
+                                                                  "widths": "on"}
+    assert info["ms_on"] < info["ms_off"]
     assert ctx.model == ("model", 0.25, 1) and ctx.tun == tun
     assert tun["width_margin"] == 1.25
+
+
+def test_learned_switches_widths_off_where_they_cannot_pay():
+    # every narrowed setting costs more than the full radius (widths saturated at r): the
+    # tuning that comes back is the starting one with the widths off (width_model 2)
+    def cost(t, model):
+        return 1.0 if t["width_model"] == 2 else 2.0 + abs(t["width_margin"] - 1.1)
+
+    ctx = FakeCtx(cost)
+    start = dict(DEFAULT, cell_ratio=0.125, points_per_cell=0.125, min_cell_ratio=0.01)
+    ctx.set_tuning(**start)
+    tun, info = at.autotune_learned(ctx, POINTS, OFFSETS, mode="radius", radius=2.0, k=64,
+                                    train=lambda c: {"samples": 1})
+    assert tun == {**start, "width_model": at.OFF} and ctx.tun == tun
+    assert info["widths"] == "off" and info["ms_off"] < info["ms_on"]
 
 
 def test_grid_of_takes_the_cell_settings():

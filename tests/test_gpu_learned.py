@@ -276,3 +276,26 @@ def _tile_widths_check(ctx, torch):
     st = rtnn_b200.Stats()
     ctx.search(p, None, "knn", 2.0, 16, learned=True, stats=st)
     assert st.n_fallback < 0.25 * p.shape[0]
+
+
+def test_widths_off_is_the_plain_search(ctx):
+    """width_model 2 switches the learned widths off: a learned search (a model loaded)
+    takes every query at the full radius -- no escalation, the plain search's rows and its
+    launch count -- and the widths the learned search reports are all r."""
+    import torch
+    base = ctx.tuning().as_dict()
+    try:
+        ctx.set_tuning(**{**base, "width_model": 0})
+        _train(ctx, epochs=2, seeds=range(20, 22), n=50_000)
+        ctx.set_tuning(**{**base, "width_model": 2})
+        p = _cloud(3, 60_000)
+        exp = oracle.grid_search(p, None, "knn", 2.0, 16)
+        st, sp = rtnn_b200.Stats(), rtnn_b200.Stats()
+        got = ctx.search(p, None, "knn", 2.0, 16, learned=True, sorted_rows=True, stats=st)
+        assert np.array_equal(got, exp)
+        ctx.search(p, None, "knn", 2.0, 16, sorted_rows=True, stats=sp)
+        assert st.n_fallback == 0 and st.n_launches == sp.n_launches
+        w = ctx.query_widths(torch.from_numpy(p).cuda(), None, "knn", 2.0, 16, learned=True)
+        assert bool((w.cpu() == 2.0).all())
+    finally:
+        ctx.set_tuning(**base)

@@ -130,7 +130,7 @@ def test_compiled_k_matches_the_generic_kernels(ctx, k):
     try:
         for mode in ("radius", "knn"):
             exp = oracle.grid_search(p, None, mode, 2.5, k)
-            for qw in (0, 1):
+            for qw in (0, 1, 3, 4):
                 for slots in (16, 20):
                     ctx.set_tuning(**{**base, "pending_slots": slots, "query_warps": qw})
                     got = ctx.search(p, None, mode, 2.5, k, sorted_rows=True)
@@ -416,11 +416,12 @@ def test_pending_slots_give_identical_rows(ctx, slots):
         ctx.set_tuning(**base)
 
 
-@pytest.mark.parametrize("qw", [1, 2])
+@pytest.mark.parametrize("qw", [1, 2, 3, 4])
 @pytest.mark.parametrize("k", [1, 5, 32, 64, 96, 128])
 def test_query_warps_match_oracle(ctx, k, qw):
     """One warp per query (query_warps 1: every pass; 2: escalation passes only; K > 64
-    falls back to the tile walk): rows equal the oracle's, sorted and as sets, with the
+    falls back to the tile walk) and the lane walk (3: first pass, one warp per query for the
+    escalations; 4: every pass): rows equal the oracle's, sorted and as sets, with the
     partition off and on (escalation passes included), in batched clouds, and with ANY_K."""
     base = ctx.tuning().as_dict()
     try:
@@ -463,7 +464,7 @@ def test_clipped_rows_keep_points_at_the_radius(ctx, cell_ratio):
     q = np.concatenate([p[::7], p[::11] + np.float32(0.125)]).astype(np.float32)
     r = float(np.nextafter(np.float32(0.75), np.float32(1)))
     try:
-        for qw in (0, 1, 2):
+        for qw in (0, 1, 2, 3, 4):
             ctx.set_tuning(**{**base, "cell_ratio": cell_ratio, "points_per_cell": 0.0,
                               "query_warps": qw})
             for mode, k in (("knn", 32), ("radius", 128)):
@@ -483,7 +484,7 @@ def test_clip_off_for_widths_beyond_the_grid(ctx):
     base = ctx.tuning().as_dict()
     u = wl.uniform_cube(2000, 1.0, seed=3)
     try:
-        for qw in (0, 1):
+        for qw in (0, 1, 4):
             ctx.set_tuning(**{**base, "cell_ratio": 0.125, "min_cell_ratio": 1e-25,
                               "points_per_cell": 0.125, "query_warps": qw})
             for mode, k in (("radius", 128), ("knn", 32), ("knn", 64)):
