@@ -16,8 +16,12 @@
 namespace rtnn {
 namespace {
 
-// Loads the points [begin, end) of one chunk into shared memory with 16-byte vector
-// loads (the AoS float3 input is read as float4 words; edges fall back to scalars).
+// Loads the points [begin, end) of one chunk into shared memory with 16-byte vector loads
+// (the AoS float3 input is read as float4 words; edge words fall back to scalars). Every
+// thread issues all of its loads before it stores any of them (kChunkWords words per
+// thread at most), so a block keeps its whole chunk in flight at once.
+constexpr int kChunkThreads = 256;
+constexpr int kChunkWords = (kChunk * 3 / 4 + 1 + kChunkThreads - 1) / kChunkThreads;   // 7
 __device__ __forceinline__ void load_chunk_xyz(const float* __restrict__ xyz, uint32_t begin,
                                                uint32_t end, uint64_t total_floats,
                                                bool aligned, float* s_xyz) {
@@ -27,13 +31,20 @@ __device__ __forceinline__ void load_chunk_xyz(const float* __restrict__ xyz, ui
     const uint64_t full_end = total_floats & ~3ull;  // words fully inside the array
     const uint64_t nw = (f1 - a0 + 3) >> 2;
     const float4* w4 = reinterpret_cast<const float4*>(xyz + a0);
-    for (uint64_t w = threadIdx.x; w < nw; w += blockDim.x) {
+    float4 v[kChunkWords];
+#pragma unroll
+    for (int u = 0; u < kChunkWords; ++u) {
+      const uint64_t w = threadIdx.x + (uint64_t)u * kChunkThreads;
       const uint64_t f = a0 + 4 * w;
-      float vals[4];
-      if (f + 4 <= full_end) {
-        float4 t = __ldg(w4 + w);
-        vals[0] = t.x; vals[1] = t.y; vals[2] = t.z; vals[3] = t.w;
-      } else {
+      v[u] = (w < nw && f + 4 <= full_end) ? __ldg(w4 + w) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < kChunkWords; ++u) {
+      const uint64_t w = threadIdx.x + (uint64_t)u * kChunkThreads;
+      if (w >= nw) continue;
+      const uint64_t f = a0 + 4 * w;
+      float vals[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+      if (f + 4 > full_end) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) vals[i] = (f + i < total_floats) ? __ldg(xyz + f + i) : 0.f;
       }
@@ -301,8 +312,11 @@ __device__ __forceinline__ uint32_t point_cell(const CloudGrid& g, float x, floa
          (uint32_t)cx;
 }
 
-// Per point: global cell id, rank within the cell from the atomic count.
-__global__ void __launch_bounds__(256)
+// Per point: global cell id, rank within the cell from the atomic count. Each thread takes
+// kChunk / 256 points of the staged chunk: all cells first, then all atomics (independent,
+// in flight together), then the ranks (coalesced).
+constexpr int kPerThread = kChunk / kChunkThreads;   // 8
+__global__ void __launch_bounds__(kChunkThreads)
 k_count(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, CloudTables t,
         const CloudGrid* __restrict__ grids, uint32_t* __restrict__ cells,
         uint32_t* __restrict__ rank, Counters* ctr) {
@@ -310,18 +324,29 @@ k_count(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Clou
   const ChunkRange r = chunk_range(t.chunk_base, t.point_off, t.n_clouds, blockIdx.x);
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
   const CloudGrid g = grids[r.cloud];
-  const uint32_t lim = g.cell_base + g.n_cells;
-  const uint32_t cap = ctr->total_cells;
-  for (uint32_t i = threadIdx.x; i < r.end - r.begin; i += blockDim.x) {
-    const uint32_t cell = point_cell(g, s_xyz[3 * i], s_xyz[3 * i + 1], s_xyz[3 * i + 2]);
-    if (cell >= lim || cell >= cap) { set_error(ctr, kErrIndexRange, r.begin + i); continue; }
-    rank[r.begin + i] = atomicAdd(&cells[cell], 1u);
+  const uint32_t lim = min(g.cell_base + g.n_cells, ctr->total_cells);
+  const uint32_t n = r.end - r.begin;
+  uint32_t cell[kPerThread];
+#pragma unroll
+  for (int u = 0; u < kPerThread; ++u) {
+    const uint32_t i = threadIdx.x + u * kChunkThreads;
+    cell[u] = i < n ? point_cell(g, s_xyz[3 * i], s_xyz[3 * i + 1], s_xyz[3 * i + 2]) : lim;
+    if (i < n && cell[u] >= lim) set_error(ctr, kErrIndexRange, r.begin + i);
+  }
+  uint32_t rk[kPerThread];
+#pragma unroll
+  for (int u = 0; u < kPerThread; ++u) rk[u] = cell[u] < lim ? atomicAdd(&cells[cell[u]], 1u) : 0u;
+#pragma unroll
+  for (int u = 0; u < kPerThread; ++u) {
+    const uint32_t i = threadIdx.x + u * kChunkThreads;
+    if (cell[u] < lim) rank[r.begin + i] = rk[u];
   }
 }
 
 // Scatter into cell-sorted float4 {x, y, z, original index}. sorted_pos (optional): the
-// inverse map, sorted_pos[original index] = position in spts.
-__global__ void __launch_bounds__(256)
+// inverse map, sorted_pos[original index] = position in spts. Per thread as in k_count:
+// every cell offset and rank is loaded before any point is written.
+__global__ void __launch_bounds__(kChunkThreads)
 k_scatter(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, CloudTables t,
           const CloudGrid* __restrict__ grids, const uint32_t* __restrict__ cells,
           const uint32_t* __restrict__ rank, float4* __restrict__ spts, uint32_t n_points,
@@ -330,16 +355,24 @@ k_scatter(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cl
   const ChunkRange r = chunk_range(t.chunk_base, t.point_off, t.n_clouds, blockIdx.x);
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
   const CloudGrid g = grids[r.cloud];
-  const uint32_t lim = g.cell_base + g.n_cells;
-  const uint32_t cap = ctr->total_cells;
-  for (uint32_t i = threadIdx.x; i < r.end - r.begin; i += blockDim.x) {
-    const float x = s_xyz[3 * i], y = s_xyz[3 * i + 1], z = s_xyz[3 * i + 2];
-    const uint32_t cell = point_cell(g, x, y, z);
-    if (cell >= lim || cell >= cap) continue;   // already reported by k_count
-    const uint32_t pos = cells[cell] + rank[r.begin + i];
-    if (pos >= n_points) { set_error(ctr, kErrIndexRange, r.begin + i); continue; }
-    spts[pos] = make_float4(x, y, z, __uint_as_float(r.begin + i));
-    if (sorted_pos) sorted_pos[r.begin + i] = pos;
+  const uint32_t lim = min(g.cell_base + g.n_cells, ctr->total_cells);
+  const uint32_t n = r.end - r.begin;
+  uint32_t pos[kPerThread];
+#pragma unroll
+  for (int u = 0; u < kPerThread; ++u) {
+    const uint32_t i = threadIdx.x + u * kChunkThreads;
+    const uint32_t cell = i < n ? point_cell(g, s_xyz[3 * i], s_xyz[3 * i + 1], s_xyz[3 * i + 2]) : lim;
+    // a point outside its grid was already reported by k_count
+    pos[u] = cell < lim ? __ldg(cells + cell) + __ldg(rank + r.begin + i) : 0xffffffffu;
+  }
+#pragma unroll
+  for (int u = 0; u < kPerThread; ++u) {
+    const uint32_t i = threadIdx.x + u * kChunkThreads;
+    if (i >= n || pos[u] == 0xffffffffu) continue;
+    if (pos[u] >= n_points) { set_error(ctr, kErrIndexRange, r.begin + i); continue; }
+    spts[pos[u]] = make_float4(s_xyz[3 * i], s_xyz[3 * i + 1], s_xyz[3 * i + 2],
+                               __uint_as_float(r.begin + i));
+    if (sorted_pos) sorted_pos[r.begin + i] = pos[u];
   }
 }
 
@@ -376,15 +409,37 @@ k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
   }
 }
 
-// Sorted queries as float4 {x, y, z, original query index} (+ their widths).
-__global__ void k_gather_queries(const float* __restrict__ xyz, const uint32_t* __restrict__ order,
-                                 uint32_t n, float4* __restrict__ sq,
-                                 const float* __restrict__ w_in, float* __restrict__ w_out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t q = order[i];
-    const float* p = xyz + 3ull * q;
-    sq[i] = make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __uint_as_float(q));
-    if (w_in) w_out[i] = __ldg(w_in + q);
+// Sorted queries as float4 {x, y, z, original query index} (+ their widths). Each thread
+// takes kGather queries a round: their order entries, then all gathers, then the stores.
+constexpr int kGather = 4;
+__global__ void __launch_bounds__(256)
+k_gather_queries(const float* __restrict__ xyz, const uint32_t* __restrict__ order, uint32_t n,
+                 float4* __restrict__ sq, const float* __restrict__ w_in, float* __restrict__ w_out) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += kGather * stride) {
+    uint32_t q[kGather];
+#pragma unroll
+    for (int u = 0; u < kGather; ++u) {
+      const uint32_t i = base + u * stride;
+      q[u] = i < n ? __ldg(order + i) : 0u;
+    }
+    float4 v[kGather];
+    float wv[kGather];
+#pragma unroll
+    for (int u = 0; u < kGather; ++u) {
+      const uint32_t i = base + u * stride;
+      const float* p = xyz + 3ull * q[u];
+      v[u] = i < n ? make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __uint_as_float(q[u]))
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
+      wv[u] = (i < n && w_in) ? __ldg(w_in + q[u]) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kGather; ++u) {
+      const uint32_t i = base + u * stride;
+      if (i >= n) continue;
+      sq[i] = v[u];
+      if (w_in) w_out[i] = wv[u];
+    }
   }
 }
 
@@ -412,7 +467,12 @@ cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const
   if (e == cudaSuccess) e = cudaMemsetAsync(bbox + 3ull * t.n_clouds, 0, 3ull * t.n_clouds * 4, s);
   if (e != cudaSuccess) return e;
   if (n_chunks == 0) return cudaSuccess;
-  const unsigned blocks = (unsigned)min((uint64_t)n_chunks, (uint64_t)n_sms * 8);
+  // one wave of resident blocks, each streaming a contiguous range of chunks
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bbox, 256, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const unsigned blocks = (unsigned)min((uint64_t)n_chunks, (uint64_t)n_sms * per_sm);
   k_bbox<<<blocks, 256, 0, s>>>(xyz, 3 * n_points, aligned, t, n_chunks, bbox);
   return cudaGetLastError();
 }
