@@ -409,6 +409,9 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
     sph = name == "sph_lattice_5e7"
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     noise = torch.empty_like(tp) if sph else None
+    # every timed block of the SPH workload starts from the same positions and noise seed,
+    # so that the plain and the learned path step through the same trajectory
+    tp0 = tp.clone() if sph else None
 
     def step(plan):
         if sph:
@@ -417,6 +420,9 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
         plan.execute(tp, tq, out)
 
     def timed(plan, n_steps, n_warm, clocks=None):
+        if sph:
+            tp.copy_(tp0)
+            gen.manual_seed(1234 + rank)
         for _ in range(n_warm):
             step(plan)
         barrier()
@@ -438,7 +444,12 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
     plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, presets=at.GRID_PRESETS,
                                use_cache=False, **common)
     plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
-    plain_ms, _ = timed(plain, steps, max(1, warmup // 2))
+    # the headline times exactly `steps` steps; the other workloads time at least ~100 ms
+    # per path (their steps take 0.2-50 ms), the same count for both paths
+    if not headline:
+        one, _ = timed(plain, 1, 1)
+        steps = int(min(200, max(steps, np.ceil(100.0 / max(one, 1e-3)))))
+    plain_ms, _ = timed(plain, steps, warmup)
     plain.close()
 
     # learned partition: starting from the plain search's tuned settings, for each
@@ -539,7 +550,7 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
             "ms_main": ms_main, "model": model_info,
             "tuning": {"learned": learned_tuning, "plain": plain_tuning},
             "roofline": roofline, "cpu": cpu, "e2e": e2e, "launches": launches_per_step,
-            "clocks": clocks}
+            "clocks": clocks, "steps": steps}
 
 
 def ctx_default_tuning(ctx):
@@ -615,7 +626,8 @@ def run_rtnn(args, rank, world):
                 "stage_ms": o["stage_ms"], "roofline": {"frac": o["roofline"]["frac"],
                                                         "achieved": o["roofline"]["achieved"],
                                                         "unit": "GB/s", "kernel": "k_search (all passes)"},
-                "cpu_baseline": o["cpu"], "tuning": o["tuning"], "steps": min(args.steps, 5)}
+                "cpu_baseline": o["cpu"], "tuning": o["tuning"], "steps": o["steps"],
+                "widths": (o["model"] or {}).get("widths")}
 
     value = world * Q / (ms_learned * 1e-3)
     line = {"metric": "queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
