@@ -111,11 +111,14 @@ struct rtnn_ctx {
   DevBuf model;
   bool has_model = false;
   DevBuf train_grad, train_m, train_v, train_loss;
-  // host-buffer batches in sub-batches (run_batched_overlapped): download stream, per
-  // sub-batch stage events, per sub-batch counters
-  cudaStream_t copy = nullptr;
-  cudaEvent_t sub_ev[8][5] = {};
+  // host-buffer batches in sub-batches (run_batched_overlapped): download and upload
+  // streams, per sub-batch stage events (the five of issue() and the upload's), per
+  // sub-batch counters
+  cudaStream_t copy = nullptr, up = nullptr;
+  cudaEvent_t sub_ev[32][6] = {};
   DevBuf sub_ctr;
+  uint32_t* h_tab = nullptr;   // pinned: every sub-batch's cloud tables, uploaded async
+  size_t h_tab_cap = 0;
   // the order of the last search in ws (rtnn_layout): valid after a one-batch search
   bool layout_valid = false;
   uint64_t layout_n = 0, layout_q = 0;
@@ -617,18 +620,23 @@ rtnn_status run_search(rtnn_ctx* c, const Shapes& sh, const Params& pr, const fl
 }
 
 // Host buffers, many clouds: the batch runs as sub-batches of whole clouds (about equal
-// query counts) on the context's stream, and a second stream downloads each sub-batch's
-// rows as soon as it is done -- the rows of consecutive clouds are contiguous and clouds
-// are independent -- so the result download (4 K bytes per query) overlaps the search of
-// the sub-batches after it. Every sub-batch is enqueued before any download, so the host
-// never waits on a download while work is still to be issued (a download into pageable
-// memory returns only once done). Same rows as one batch; stats are summed.
-constexpr uint32_t kMaxSub = 8;
+// query counts) on the context's stream; a second stream uploads each sub-batch's points
+// (and queries) ahead of its search, and a third downloads each sub-batch's rows as soon
+// as it is done -- the rows of consecutive clouds are contiguous and clouds are
+// independent -- so the uploads, the searches and the result download (4 K bytes per
+// query, the bound of the call) all overlap; only the first sub-batch's upload and search
+// and the last one's download are exposed, hence many small sub-batches. Every upload and
+// sub-batch is enqueued before any download, so the host never waits on a download while
+// work is still to be issued (a copy to or from pageable memory returns only once done).
+// Same rows as one batch; stats are summed.
+constexpr uint32_t kMaxSub = 10;
 constexpr uint64_t kOverlapMinBytes = 256ull << 20;   // smaller outputs: one batch
+constexpr uint64_t kSubRowBytes = 128ull << 20;       // rows per sub-batch (about)
 
 uint32_t overlap_sub_batches(uint64_t out_bytes, uint32_t n_clouds) {
   if (out_bytes < kOverlapMinBytes || n_clouds < 2) return 1;
-  return (uint32_t)std::min<uint64_t>({kMaxSub, n_clouds, std::max<uint64_t>(2, out_bytes / (256ull << 20))});
+  return (uint32_t)std::min<uint64_t>(
+      {kMaxSub, n_clouds, std::max<uint64_t>(2, out_bytes / kSubRowBytes)});
 }
 
 rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_clouds,
@@ -665,26 +673,76 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
   }
   cudaStream_t s = stream_of(c);
   if (!c->copy) RTNN_CU(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking), "create stream");
+  if (!c->up) RTNN_CU(cudaStreamCreateWithFlags(&c->up, cudaStreamNonBlocking), "create stream");
   for (auto& row : c->sub_ev)
     for (auto& e : row)
-      if (!e) RTNN_CU(cudaEventCreate(&e), "create event");
+      if (!e) RTNN_CU(cudaEventCreateWithFlags(&e, cudaEventDefault), "create event");
   const size_t out_bytes = (size_t)Q * pr.k * sizeof(int32_t);
   RTNN_CU(ensure(c->ws.in_pts, std::max<uint64_t>(N, 1) * 12), "alloc points");
   RTNN_CU(ensure(c->ws.out, out_bytes), "alloc output");
   RTNN_CU(ensure(c->sub_ctr, (size_t)kMaxSub * sizeof(Counters)), "alloc counters");
-  RTNN_CU(cudaMemcpyAsync(c->ws.in_pts.p, points, N * 12, cudaMemcpyHostToDevice, s), "copy points");
   const float* d_pts = (const float*)c->ws.in_pts.p;
   const float* d_qs = d_pts;
   if (queries) {
     RTNN_CU(ensure(c->ws.in_qs, Q * 12), "alloc queries");
-    RTNN_CU(cudaMemcpyAsync(c->ws.in_qs.p, queries, Q * 12, cudaMemcpyHostToDevice, s), "copy queries");
     d_qs = (const float*)c->ws.in_qs.p;
+  }
+  // uploads on their own stream, in sub-batch order, after the work already on the
+  // context's stream (which may still read these buffers)
+  RTNN_CU(cudaEventRecord(c->sub_ev[0][5], s), "event");
+  RTNN_CU(cudaStreamWaitEvent(c->up, c->sub_ev[0][5], 0), "wait");
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint64_t p0 = point_off[cut[g]], np = point_off[cut[g + 1]] - p0;
+    if (np)
+      RTNN_CU(cudaMemcpyAsync((char*)c->ws.in_pts.p + p0 * 12, points + 3 * p0, np * 12,
+                              cudaMemcpyHostToDevice, c->up),
+              "copy points");
+    if (queries) {
+      const uint64_t q0 = qoff[cut[g]], nq = qoff[cut[g + 1]] - q0;
+      if (nq)
+        RTNN_CU(cudaMemcpyAsync((char*)c->ws.in_qs.p + q0 * 12, queries + 3 * q0, nq * 12,
+                                cudaMemcpyHostToDevice, c->up),
+                "copy queries");
+    }
+    RTNN_CU(cudaEventRecord(c->sub_ev[g][5], c->up), "event");
   }
   int32_t* d_out = (int32_t*)c->ws.out.p;
   Counters* d_sub = (Counters*)c->sub_ctr.p;
+  // the cloud tables of every sub-batch in pinned memory, so that their uploads never make
+  // the host wait for the stream (a copy from pageable memory may)
+  size_t tab_words = 0;
+  for (const Shapes& sh : shs) tab_words += sh.tab.size();
+  if (tab_words > c->h_tab_cap) {
+    if (c->h_tab) cudaFreeHost(c->h_tab);
+    c->h_tab = nullptr;
+    c->h_tab_cap = 0;
+    RTNN_CU(cudaMallocHost((void**)&c->h_tab, tab_words * 4), "alloc pinned tables");
+    c->h_tab_cap = tab_words;
+  }
+  // downloads into page-locked memory are asynchronous: each is enqueued right after its
+  // sub-batch; into pageable memory after the last sub-batch (such a download returns only
+  // once done, and the host must first have issued all the work)
+  cudaPointerAttributes oattr{};
+  const bool out_pinned = cudaPointerGetAttributes(&oattr, out) == cudaSuccess &&
+                          oattr.type == cudaMemoryTypeHost;
+  cudaGetLastError();   // clear a failed attribute query of pageable memory
+  auto download = [&](uint32_t g) -> rtnn_status {
+    RTNN_CU(cudaStreamWaitEvent(c->copy, c->sub_ev[g][4], 0), "wait");
+    const uint64_t q0 = qoff[cut[g]], nq = qoff[cut[g + 1]] - q0;
+    if (nq)
+      RTNN_CU(cudaMemcpyAsync(out + q0 * pr.k, d_out + q0 * pr.k, nq * pr.k * 4, cudaMemcpyDeviceToHost,
+                              c->copy),
+              "copy output");
+    return RTNN_OK;
+  };
+  size_t tab_at = 0;
   for (uint32_t g = 0; g < G; ++g) {
     const Shapes& sh = shs[g];
-    RTNN_CU(cudaMemcpyAsync(c->ws.tables.p, sh.tab.data(), sh.tab.size() * 4, cudaMemcpyHostToDevice, s),
+    uint32_t* htab = c->h_tab + tab_at;
+    tab_at += sh.tab.size();
+    std::memcpy(htab, sh.tab.data(), sh.tab.size() * 4);
+    RTNN_CU(cudaStreamWaitEvent(s, c->sub_ev[g][5], 0), "wait");
+    RTNN_CU(cudaMemcpyAsync(c->ws.tables.p, htab, sh.tab.size() * 4, cudaMemcpyHostToDevice, s),
             "copy tables");
     if (sh.N == 0 || sh.Q == 0) {   // nothing to search: empty rows (if any), no counts
       if (sh.Q)
@@ -699,14 +757,14 @@ rtnn_status run_batched_overlapped(rtnn_ctx* c, const uint64_t* point_off, uint3
       RTNN_CU(cudaMemcpyAsync(d_sub + g, c->ws.counters.p, sizeof(Counters), cudaMemcpyDeviceToDevice, s),
               "save counters");
     }
+    if (out_pinned) {
+      const rtnn_status st = download(g);
+      if (st != RTNN_OK) return st;
+    }
   }
-  for (uint32_t g = 0; g < G; ++g) {   // each download after its sub-batch's last event
-    RTNN_CU(cudaStreamWaitEvent(c->copy, c->sub_ev[g][4], 0), "wait");
-    const uint64_t q0 = qoff[cut[g]], nq = qoff[cut[g + 1]] - q0;
-    if (nq)
-      RTNN_CU(cudaMemcpyAsync(out + q0 * pr.k, d_out + q0 * pr.k, nq * pr.k * 4, cudaMemcpyDeviceToHost,
-                              c->copy),
-              "copy output");
+  for (uint32_t g = 0; g < G && !out_pinned; ++g) {   // each after its sub-batch's last event
+    const rtnn_status st = download(g);
+    if (st != RTNN_OK) return st;
   }
   RTNN_CU(cudaStreamSynchronize(c->copy), "synchronize");
   std::vector<Counters> h(G);
@@ -814,6 +872,8 @@ rtnn_status rtnn_destroy(rtnn_ctx* c) {
       if (e) cudaEventDestroy(e);
   release(c->sub_ctr);
   if (c->copy) cudaStreamDestroy(c->copy);
+  if (c->up) cudaStreamDestroy(c->up);
+  if (c->h_tab) cudaFreeHost(c->h_tab);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
   if (c->h_grid) cudaFreeHost(c->h_grid);
   if (c->own) cudaStreamDestroy(c->own);
