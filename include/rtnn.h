@@ -220,6 +220,11 @@ typedef struct rtnn_tuning {
                                  K-th distances at r, or a grid already tight around them).
                                  The model is trained for one kind (rtnn_collect_training
                                  follows this setting; 2 collects per-query samples) */
+  uint32_t width_clip;        /* partitioned search, tile walk: in each run of a tile the
+                                 `width_clip` widest narrowed widths are clipped to the next
+                                 widest, so one outlier does not grow the shared candidate box;
+                                 a clipped query that finds fewer than K is escalated like any
+                                 short one, so rows stay exact (0..16; 0: no clipping) */
 } rtnn_tuning;
 
 rtnn_status rtnn_get_tuning(const rtnn_ctx* ctx, rtnn_tuning* tuning);

@@ -79,7 +79,8 @@ class Tuning(ctypes.Structure):
                 ("width_margin", ctypes.c_float), ("fallback_passes", ctypes.c_uint32),
                 ("lane_walk_ratio", ctypes.c_float), ("gap_ratio", ctypes.c_float),
                 ("pending_slots", ctypes.c_uint32), ("query_warps", ctypes.c_uint32),
-                ("buckets_per_halving", ctypes.c_float), ("width_model", ctypes.c_uint32)]
+                ("buckets_per_halving", ctypes.c_float), ("width_model", ctypes.c_uint32),
+                ("width_clip", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -51,6 +51,7 @@ GRID_PRESETS = [
 LEARNED_KNOBS = [
     ("width_margin", [0.8, 0.9, 1.0, 1.08, 1.15, 1.25]),
     ("fallback_passes", [2, 4, 6]),
+    ("width_clip", [0, 2, 4, 8]),
 ]
 
 

@@ -103,7 +103,7 @@ struct rtnn_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.1f, 4u, 0.0f, 2.0f, 16u, 2u, 1.0f, 0u};
+  rtnn_tuning tuning{0.5f, 0.0625f, 0.f, 16.f, 4u, 0u, 1.1f, 4u, 0.0f, 2.0f, 16u, 2u, 1.0f, 0u, 0u};
   Workspace ws;
   cudaEvent_t ev[6] = {};
   Counters* h_ctr = nullptr;   // pinned
@@ -441,6 +441,7 @@ rtnn_status issue(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& pr
   a.index_base = index_base;
   a.ref_ppos = ref_layout ? (const uint32_t*)ws.ppos.p : nullptr;
   a.lane_walk_ratio = tu.lane_walk_ratio;
+  a.width_clip = tu.width_clip;
   a.gap_ratio = tu.gap_ratio;
   a.flags = ((pr.flags & RTNN_FLAG_SORTED_ROWS) ? kSearchSortedRows : 0u) |
             ((pr.flags & RTNN_FLAG_LOCAL_INDICES) ? kSearchLocalIndices : 0u) |
@@ -903,7 +904,8 @@ rtnn_status rtnn_set_tuning(rtnn_ctx* c, const rtnn_tuning* t) {
       t->warps_per_block < 1 || t->warps_per_block > 8 || !(t->width_margin > 0.f) ||
       !(t->lane_walk_ratio >= 0.f) || !(t->gap_ratio >= 0.f) || t->pending_slots < 8 ||
       t->pending_slots > 256 || t->query_warps > 4 ||
-      !(t->buckets_per_halving >= 0.f && t->buckets_per_halving <= 8.f) || t->width_model > 2)
+      !(t->buckets_per_halving >= 0.f && t->buckets_per_halving <= 8.f) || t->width_model > 2 ||
+      t->width_clip > 16)
     return fail(c, RTNN_ERR_INVALID_ARGUMENT, "tuning values out of range");
   c->tuning = *t;
   return RTNN_OK;

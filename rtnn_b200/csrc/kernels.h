@@ -50,6 +50,8 @@ struct SearchArgs {
   float* width_out;            // optional: the main-pass width of each query (query index)
   int pass;                    // kPassMain, kPassEscalate or kPassFinal
   float lane_walk_ratio;       // tile spread > ratio * width: per-lane walk (0: never)
+  uint32_t width_clip;         // tile walk, flagging passes: the widest widths of a run
+                               // clipped to the (width_clip + 1)-th widest (0: none)
   float gap_ratio;             // split a tile where consecutive queries are farther apart
                                // than ratio * width (0: split at cloud changes only)
 };

@@ -450,6 +450,30 @@ k_search(SearchArgs a) {
       const uint32_t gcloud = __shfl_sync(0xffffffffu, cloud, leader);
       pending &= ~group;
       const bool act = (group >> lane) & 1u;
+      if constexpr (!LANES) {
+        // width clip (flagging passes only, whose short queries are searched again): the
+        // run's widest widths are clipped to the (width_clip + 1)-th widest, at most a
+        // quarter of the run, so that the candidate box follows the bulk of the run
+        const uint32_t n_act = __popc(group);
+        const uint32_t rank = min(a.width_clip, n_act / 4u);
+        if (rank > 0 && a.fb_flag && a.pass != kPassFinal) {
+          float v = act ? w : -INFINITY;   // bitonic sort, ascending over the lanes
+#pragma unroll
+          for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+              const float o = __shfl_xor_sync(0xffffffffu, v, stride);
+              const bool up = (lane & size) == 0, low = (lane & stride) == 0;
+              v = (low == up) ? fminf(v, o) : fmaxf(v, o);
+            }
+          }
+          const float wc = __shfl_sync(0xffffffffu, v, 31 - (int)rank);
+          if (act && w > wc) {
+            w = wc;
+            lim = __fmul_rn(wc, wc);
+          }
+        }
+      }
 
       // 1. group bounding box and widest width
       const float bx0 = wmin(act ? q.x : INFINITY), bx1 = wmax(act ? q.x : -INFINITY);

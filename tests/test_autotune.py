@@ -16,7 +16,7 @@ from rtnn_b200 import autotune as at
 DEFAULT = dict(cell_ratio=0.5, min_cell_ratio=0.0625, points_per_cell=0.0, cell_budget=16.0,
                warps_per_block=4, blocks_per_sm=0, width_margin=1.1, fallback_passes=4,
                lane_walk_ratio=0.0, gap_ratio=2.0, pending_slots=16, query_warps=2,
-               buckets_per_halving=1.0, width_model=0)
+               buckets_per_halving=1.0, width_model=0, width_clip=0)
 
 
 class _Tuning(dict):
@@ -54,7 +54,7 @@ class FakeCtx:
               kw["points_per_cell"] >= 0 and 1 <= kw["warps_per_block"] <= 8 and
               8 <= kw["pending_slots"] <= 256 and kw["query_warps"] <= 4 and
               kw["fallback_passes"] <= 6 and 0 <= kw["buckets_per_halving"] <= 8 and
-              kw["width_model"] <= 2)
+              kw["width_model"] <= 2 and kw["width_clip"] <= 16)
         if not ok:
             self.rejected += 1
             raise rtnn_b200.RtnnError(1, "tuning values out of range")

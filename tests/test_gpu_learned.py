@@ -299,3 +299,36 @@ def test_widths_off_is_the_plain_search(ctx):
         assert bool((w.cpu() == 2.0).all())
     finally:
         ctx.set_tuning(**base)
+
+
+@pytest.mark.parametrize("clip", [2, 8, 16])
+def test_width_clip_stays_exact(ctx, clip):
+    """rtnn_tuning.width_clip: the widest per-query widths of a tile run are clipped to the
+    next widest; a clipped query that finds fewer than K is escalated, so the rows equal the
+    oracle's, and no fewer queries are escalated than without the clip."""
+    base = ctx.tuning().as_dict()
+    try:
+        ctx.set_tuning(**{**base, "width_model": 0, "width_clip": 0})
+        _train(ctx, epochs=3, seeds=range(20, 23), n=60_000)
+        p = _cloud(4, 80_000)
+        exp = oracle.grid_search(p, None, "knn", 2.0, 16)
+        st0, st = rtnn_b200.Stats(), rtnn_b200.Stats()
+        ctx.search(p, None, "knn", 2.0, 16, learned=True, stats=st0)
+        ctx.set_tuning(**{**base, "width_model": 0, "width_clip": clip})
+        for kw in ({"learned": True}, {"partition": True}):
+            got = ctx.search(p, None, "knn", 2.0, 16, sorted_rows=True, stats=st, **kw)
+            assert np.array_equal(got, exp)
+        got = ctx.search(p, None, "knn", 2.0, 16, learned=True, stats=st)
+        assert_sets = np.sort(np.where(got < 0, 1 << 30, got), 1)
+        assert np.array_equal(assert_sets, np.sort(np.where(exp < 0, 1 << 30, exp), 1))
+        assert st.n_fallback >= st0.n_fallback
+        # the radius mode and the multi-cloud path with the clip
+        r_exp = oracle.grid_search(p, None, "radius", 1.5, 32)
+        assert np.array_equal(ctx.search(p, None, "radius", 1.5, 32, partition=True,
+                                         sorted_rows=True), r_exp)
+        q, off = wl.multicloud(n_clouds=12, lo=64, hi=3000, seed=9)
+        got = ctx.search_batched(q, off, mode="knn", radius=0.2, k=32, sorted_rows=True,
+                                 partition=True)
+        assert np.array_equal(got, oracle.grid_search_batched(q, off, mode="knn", r=0.2, k=32))
+    finally:
+        ctx.set_tuning(**base)
