@@ -398,14 +398,26 @@ k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
   const CloudGrid g = grids[r.cloud];
   const int top = (int)((1u << order_bits) - 1u);
-  for (uint32_t i = threadIdx.x; i < r.end - r.begin; i += blockDim.x) {
+  const uint32_t n = r.end - r.begin;
+  // the widths of this thread's queries are loaded before any key is computed
+  uint32_t lvl[kPerThread];
+#pragma unroll
+  for (int u = 0; u < kPerThread; ++u) {
+    const uint32_t i = threadIdx.x + u * kChunkThreads;
+    lvl[u] = (qwidth && i < n) ? width_level(__ldg(qwidth + r.begin + i), radius, level_bits,
+                                             per_halving)
+                               : 0u;
+  }
+#pragma unroll 2
+  for (int u = 0; u < kPerThread; ++u) {
+    const uint32_t i = threadIdx.x + u * kChunkThreads;
+    if (i >= n) break;
     const int fx = clamp_cell(cell_coord_f(s_xyz[3 * i], g.ox, g.order_scale), top + 1);
     const int fy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.order_scale), top + 1);
     const int fz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.order_scale), top + 1);
     const uint64_t m = hilbert3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz, order_bits);
-    const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits, per_halving) : 0u;
     keys[r.begin + i] = ((KeyT)r.cloud << (3 * order_bits + level_bits)) |
-                        ((KeyT)lvl << (3 * order_bits)) | (KeyT)m;
+                        ((KeyT)lvl[u] << (3 * order_bits)) | (KeyT)m;
   }
 }
 
@@ -467,12 +479,9 @@ cudaError_t launch_bbox(const float* xyz, uint64_t n_points, bool aligned, const
   if (e == cudaSuccess) e = cudaMemsetAsync(bbox + 3ull * t.n_clouds, 0, 3ull * t.n_clouds * 4, s);
   if (e != cudaSuccess) return e;
   if (n_chunks == 0) return cudaSuccess;
-  // one wave of resident blocks, each streaming a contiguous range of chunks
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bbox, 256, 0) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  const unsigned blocks = (unsigned)min((uint64_t)n_chunks, (uint64_t)n_sms * per_sm);
+  // eight blocks per SM, each streaming a contiguous range of chunks (measured faster than
+  // one wave of resident blocks: 257 against 270 us for 54.8 M points)
+  const unsigned blocks = (unsigned)min((uint64_t)n_chunks, (uint64_t)n_sms * 8);
   k_bbox<<<blocks, 256, 0, s>>>(xyz, 3 * n_points, aligned, t, n_chunks, bbox);
   return cudaGetLastError();
 }
