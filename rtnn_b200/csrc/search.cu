@@ -919,6 +919,92 @@ __device__ __noinline__ uint64_t warp_select(uint64_t* buf, uint32_t n, uint32_t
   return warp_sort_keep<4>(buf, n, keep);
 }
 
+// Keeps the `keep` smallest of buf[0, n) (keep < n <= 128) at buf[0, keep), in no
+// particular order, and returns the largest kept key. Instead of sorting, the warp finds a
+// threshold on the distance bits with exactly `keep` keys below it: every count is one
+// ballot per held key (up to four per lane), the first probe is a guess -- within a ball the
+// count grows as d^(3/2), so the keep-th distance lies about (2/3) log2(n / keep) octaves
+// below the largest, a fixed offset on the float bits -- and the rest bisect on the bits.
+// Equal distances straddling the keep-th place (lattices) are settled on the index by the
+// same count-and-bisect over the indices at that distance. The kept keys are then compacted
+// to the front with ballots. Out of line, like warp_select.
+__device__ __noinline__ uint64_t warp_threshold_keep(uint64_t* buf, uint32_t n, uint32_t keep) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = lanemask_lt();
+  uint64_t v[4];
+  uint32_t lo = 0xffffffffu, hi = 0u;
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint32_t p = (uint32_t)(e * 32 + lane);
+    v[e] = p < n ? buf[p] : ~0ull;
+    if (p < n) {
+      const uint32_t d = (uint32_t)(v[e] >> 32);
+      lo = min(lo, d);
+      hi = max(hi, d);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  // keys whose distance bits are below t (padding ~0 never counts: its bits exceed any t)
+  auto count_below = [&](uint32_t t) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) c += __popc(__ballot_sync(0xffffffffu, (uint32_t)(v[e] >> 32) < t));
+    return c;
+  };
+  // invariant: count_below(L) < keep < count_below(H); hi + 1 <= 0x7f800000 (finite d)
+  uint32_t L = lo, H = hi + 1u, T = 0u;
+  const float drop = -0.6667f * __log2f((float)keep / (float)n) * 8388608.f;
+  uint32_t t = hi - min((uint32_t)drop, hi - lo);
+  while (true) {
+    if (t <= L || t >= H) t = L + ((H - L) >> 1);
+    if (t == L) break;   // H == L + 1: the keep-th place falls among equal distances L
+    const uint32_t c = count_below(t);
+    if (c == keep) { T = t; break; }
+    if (c < keep) L = t; else H = t;
+    t = L + ((H - L) >> 1);
+  }
+  const bool tie = T == 0u;
+  uint32_t tie_idx = 0u;   // tie: keys at distance L with an index below tie_idx are kept
+  if (tie) {
+    T = L;
+    const uint32_t need = keep - count_below(L);
+    uint64_t IL = 0, IH = 0x100000000ull;   // indices differ: the count reaches `need`
+    while (IH - IL > 1) {
+      const uint64_t mid = IL + ((IH - IL) >> 1);
+      uint32_t c = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        c += __popc(__ballot_sync(0xffffffffu, (uint32_t)(v[e] >> 32) == T && (uint32_t)v[e] < mid));
+      if (c == need) { IL = mid; break; }
+      if (c < need) IL = mid; else IH = mid;
+    }
+    tie_idx = (uint32_t)IL;
+  }
+  __syncwarp();
+  uint32_t base = 0;
+  uint64_t top = 0;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint32_t d = (uint32_t)(v[e] >> 32);
+    const bool kept = d < T || (tie && d == T && (uint32_t)v[e] < tie_idx);
+    const uint32_t m = __ballot_sync(0xffffffffu, kept);
+    if (kept) {
+      buf[base + __popc(m & lt)] = v[e];
+      top = max(top, v[e]);
+    }
+    base += __popc(m);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
+  __syncwarp();
+  return top;
+}
+
 // KC > 0: K == KC compiled in (as for k_search).
 template <bool KNN, int KC>
 // three blocks per SM (80 registers): the walk is latency-bound, more resident warps
@@ -1079,7 +1165,7 @@ k_search_q(SearchArgs a) {
             if (nb >= k) { stop = true; break; }
           } else if (nb > cap - 64) {
             // keep the k nearest; later hits must beat the k-th (ties may win on index)
-            const uint64_t kth = warp_select(buf, nb, k);
+            const uint64_t kth = warp_threshold_keep(buf, nb, k);
             nb = k;
             hit_window(true, limj, __uint_as_float((uint32_t)(kth >> 32)), KNN, wlo, wspan);
           }
@@ -1098,8 +1184,10 @@ k_search_q(SearchArgs a) {
       }
       if (any_k) {   // the first k found, in the order found (sorted on request)
         if (sorted_rows && found > 1) warp_select(buf, found, found);
-      } else if (nb > k || (sorted_rows && nb > 1)) {
+      } else if (sorted_rows && nb > 1) {
         warp_select(buf, nb, found);
+      } else if (nb > k) {
+        warp_threshold_keep(buf, nb, k);
       }
       __syncwarp();
       const uint32_t sub = local_idx ? a.t.point_off[cj] : 0u - a.index_base;

@@ -467,11 +467,14 @@ def test_clipped_rows_keep_points_at_the_radius(ctx, cell_ratio):
         for qw in (0, 1, 2, 3, 4):
             ctx.set_tuning(**{**base, "cell_ratio": cell_ratio, "points_per_cell": 0.0,
                               "query_warps": qw})
-            for mode, k in (("knn", 32), ("radius", 128)):
+            for mode, k in (("knn", 32), ("radius", 128), ("knn", 20)):
                 exp = oracle.grid_search(p, q, mode, r, k)
                 for part in (False, True):
                     got = ctx.search(p, q, mode, r, k, partition=part, sorted_rows=True)
                     assert_rows_equal(got, exp, True)
+                    # unsorted rows: the K kept among lattice ties at equal distances
+                    got = ctx.search(p, q, mode, r, k, partition=part)
+                    assert_rows_equal(got, exp, False)
     finally:
         ctx.set_tuning(**base)
 
