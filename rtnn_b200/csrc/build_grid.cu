@@ -362,8 +362,11 @@ k_scatter(const float* __restrict__ xyz, uint64_t total_floats, bool aligned, Cl
   for (int u = 0; u < kPerThread; ++u) {
     const uint32_t i = threadIdx.x + u * kChunkThreads;
     const uint32_t cell = i < n ? point_cell(g, s_xyz[3 * i], s_xyz[3 * i + 1], s_xyz[3 * i + 2]) : lim;
-    // a point outside its grid was already reported by k_count
-    pos[u] = cell < lim ? __ldg(cells + cell) + __ldg(rank + r.begin + i) : 0xffffffffu;
+    // a point outside its grid was already reported by k_count; both loads stay in bounds
+    // whatever the point (cells holds total_cells + 1 entries, i is clamped to the chunk)
+    const uint32_t off = __ldg(cells + min(cell, lim));
+    const uint32_t rk = __ldg(rank + r.begin + min(i, n - 1));
+    pos[u] = cell < lim ? off + rk : 0xffffffffu;
   }
 #pragma unroll
   for (int u = 0; u < kPerThread; ++u) {
@@ -398,26 +401,14 @@ k_query_keys(const float* __restrict__ xyz, uint64_t total_floats, bool aligned,
   load_chunk_xyz(xyz, r.begin, r.end, total_floats, aligned, s_xyz);
   const CloudGrid g = grids[r.cloud];
   const int top = (int)((1u << order_bits) - 1u);
-  const uint32_t n = r.end - r.begin;
-  // the widths of this thread's queries are loaded before any key is computed
-  uint32_t lvl[kPerThread];
-#pragma unroll
-  for (int u = 0; u < kPerThread; ++u) {
-    const uint32_t i = threadIdx.x + u * kChunkThreads;
-    lvl[u] = (qwidth && i < n) ? width_level(__ldg(qwidth + r.begin + i), radius, level_bits,
-                                             per_halving)
-                               : 0u;
-  }
-#pragma unroll 2
-  for (int u = 0; u < kPerThread; ++u) {
-    const uint32_t i = threadIdx.x + u * kChunkThreads;
-    if (i >= n) break;
+  for (uint32_t i = threadIdx.x; i < r.end - r.begin; i += blockDim.x) {
     const int fx = clamp_cell(cell_coord_f(s_xyz[3 * i], g.ox, g.order_scale), top + 1);
     const int fy = clamp_cell(cell_coord_f(s_xyz[3 * i + 1], g.oy, g.order_scale), top + 1);
     const int fz = clamp_cell(cell_coord_f(s_xyz[3 * i + 2], g.oz, g.order_scale), top + 1);
     const uint64_t m = hilbert3_64((uint32_t)fx, (uint32_t)fy, (uint32_t)fz, order_bits);
+    const uint32_t lvl = qwidth ? width_level(qwidth[r.begin + i], radius, level_bits, per_halving) : 0u;
     keys[r.begin + i] = ((KeyT)r.cloud << (3 * order_bits + level_bits)) |
-                        ((KeyT)lvl[u] << (3 * order_bits)) | (KeyT)m;
+                        ((KeyT)lvl << (3 * order_bits)) | (KeyT)m;
   }
 }
 
@@ -436,21 +427,22 @@ k_gather_queries(const float* __restrict__ xyz, const uint32_t* __restrict__ ord
       q[u] = i < n ? __ldg(order + i) : 0u;
     }
     float4 v[kGather];
-    float wv[kGather];
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
-      const uint32_t i = base + u * stride;
-      const float* p = xyz + 3ull * q[u];
-      v[u] = i < n ? make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __uint_as_float(q[u]))
-                   : make_float4(0.f, 0.f, 0.f, 0.f);
-      wv[u] = (i < n && w_in) ? __ldg(w_in + q[u]) : 0.f;
+      const float* p = xyz + 3ull * q[u];   // q[u] == 0 past the end: an in-bounds address
+      v[u] = make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __uint_as_float(q[u]));
     }
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
       const uint32_t i = base + u * stride;
-      if (i >= n) continue;
-      sq[i] = v[u];
-      if (w_in) w_out[i] = wv[u];
+      if (i < n) sq[i] = v[u];
+    }
+    if (w_in) {
+#pragma unroll
+      for (int u = 0; u < kGather; ++u) {
+        const uint32_t i = base + u * stride;
+        if (i < n) w_out[i] = w_in[q[u]];
+      }
     }
   }
 }
