@@ -71,7 +71,8 @@ struct Shapes {
   uint32_t n_clouds = 1;
   uint64_t N = 0, Q = 0;
   bool single = true;
-  std::vector<uint32_t> tab;  // batched: point_off | query_off | chunk_base | qchunk_base | tile_base
+  std::vector<uint32_t> tab;  // batched: point_off | query_off | chunk_base | qchunk_base |
+                              // tile_base | lead_base
   uint32_t n_chunks = 0, n_qchunks = 0, n_tiles = 0;
   uint64_t max_cloud_q = 0;
   uint32_t order_bits = 1, key_bits = 8;
@@ -225,13 +226,14 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
   const uint32_t n1 = n_clouds + 1;
   sh.n_clouds = n_clouds;
   sh.single = false;
-  sh.tab.assign(5ull * n1, 0u);
+  sh.tab.assign(6ull * n1, 0u);
   uint32_t* po = sh.tab.data();
   uint32_t* qo = po + n1;
   uint32_t* cb = qo + n1;
   uint32_t* qb = cb + n1;
   uint32_t* tb = qb + n1;
-  uint64_t chunks = 0, qchunks = 0, tiles = 0, maxq = 0;
+  uint32_t* lb = tb + n1;
+  uint64_t chunks = 0, qchunks = 0, tiles = 0, leads = 0, maxq = 0;
   for (uint32_t i = 0; i < n_clouds; ++i) {
     if (point_off[i + 1] < point_off[i] || qoff[i + 1] < qoff[i])
       return fail(c, RTNN_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
@@ -241,9 +243,11 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
     cb[i] = (uint32_t)chunks;
     qb[i] = (uint32_t)qchunks;
     tb[i] = (uint32_t)tiles;
+    lb[i] = (uint32_t)leads;
     chunks += (np + kChunk - 1) / kChunk;
     qchunks += (nq + kChunk - 1) / kChunk;
     tiles += (nq + kTile - 1) / kTile;
+    leads += lead_tiles((uint32_t)((nq + kTile - 1) / kTile));
     maxq = std::max(maxq, nq);
   }
   sh.N = point_off[n_clouds];
@@ -255,6 +259,7 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
   cb[n_clouds] = (uint32_t)chunks;
   qb[n_clouds] = (uint32_t)qchunks;
   tb[n_clouds] = (uint32_t)tiles;
+  lb[n_clouds] = (uint32_t)leads;
   sh.n_chunks = (uint32_t)chunks;
   sh.n_qchunks = (uint32_t)qchunks;
   sh.n_tiles = (uint32_t)tiles;
@@ -283,7 +288,7 @@ rtnn_status reserve(rtnn_ctx* c, Workspace& ws, const Shapes& sh, const Params& 
   const uint64_t N = std::max<uint64_t>(sh.N, 1), Q = std::max<uint64_t>(sh.Q, 1);
   const uint64_t rt = radix_tiles_for(Q);
   const uint64_t scan_n = std::max<uint64_t>(std::max<uint64_t>(sh.cell_capacity + 1, 256ull * rt), Q + 1);
-  RTNN_CU(ensure(ws.tables, 5 * n1 * 4), "alloc tables");
+  RTNN_CU(ensure(ws.tables, 6 * n1 * 4), "alloc tables");
   RTNN_CU(ensure(ws.grids, sh.n_clouds * sizeof(CloudGrid)), "alloc grids");
   RTNN_CU(ensure(ws.bbox, 6ull * sh.n_clouds * 4), "alloc bbox");
   RTNN_CU(ensure(ws.cells, (sh.cell_capacity + 1) * 4), "alloc cells");
@@ -321,6 +326,7 @@ CloudTables tables_of(const Workspace& ws, uint32_t n_clouds) {
   ct.chunk_base = t + 2 * n1;
   ct.qchunk_base = t + 3 * n1;
   ct.tile_base = t + 4 * n1;
+  ct.lead_base = t + 5 * n1;
   ct.n_clouds = n_clouds;
   return ct;
 }

@@ -450,11 +450,13 @@ k_gather_queries(const float* __restrict__ xyz, const uint32_t* __restrict__ ord
 // Tables of a single cloud written on the device (no host copy per call).
 __global__ void k_single_tables(uint32_t* tab, uint32_t n_points, uint32_t n_queries) {
   // tab layout: point_off[2] query_off[2] chunk_base[2] qchunk_base[2] tile_base[2]
+  // lead_base[2]
   tab[0] = 0; tab[1] = n_points;
   tab[2] = 0; tab[3] = n_queries;
   tab[4] = 0; tab[5] = (n_points + kChunk - 1) / kChunk;
   tab[6] = 0; tab[7] = (n_queries + kChunk - 1) / kChunk;
   tab[8] = 0; tab[9] = (n_queries + kTile - 1) / kTile;
+  tab[10] = 0; tab[11] = lead_tiles(tab[9]);
 }
 
 }  // namespace

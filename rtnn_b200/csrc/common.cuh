@@ -66,8 +66,19 @@ struct CloudTables {
   const uint32_t* chunk_base;  // first point chunk of cloud c; [n] = point chunks
   const uint32_t* qchunk_base; // first query chunk of cloud c; [n] = query chunks
   const uint32_t* tile_base;   // first 32-query tile of cloud c; [n] = tiles
+  const uint32_t* lead_base;   // lead tiles before cloud c; [n] = all lead tiles (below)
   uint32_t n_clouds;
 };
+
+// The lead tiles of a cloud are the first eighth of its tiles (rounded up): the queries
+// are sorted widest width bucket first, so they hold the cloud's widest searches -- the
+// longest tiles by far (up to a few ms where a wide box reaches a dense blob). The first
+// search pass takes the lead tiles of every cloud before any other tile, so that no long
+// tile starts near the end of the pass and holds it while the other SMs are idle.
+constexpr uint32_t kLeadShift = 3;
+__host__ __device__ __forceinline__ uint32_t lead_tiles(uint32_t tiles) {
+  return (tiles + (1u << kLeadShift) - 1u) >> kLeadShift;
+}
 
 __device__ __forceinline__ void set_error(Counters* c, uint32_t code, uint32_t info) {
   if (atomicCAS(&c->error, 0u, code) == 0u) c->error_info = info;
@@ -82,6 +93,29 @@ __device__ __forceinline__ uint32_t find_cloud(const uint32_t* base, uint32_t n_
     if (__ldg(base + mid) <= x) lo = mid; else hi = mid;
   }
   return lo;
+}
+
+// Work item w of the first search pass -> (cloud, tile j of that cloud): items
+// [0, lead_base[n]) are the clouds' lead tiles in cloud order, the rest their other tiles
+// in cloud order.
+__device__ __forceinline__ void main_tile(const CloudTables& t, uint32_t w, uint32_t& cloud,
+                                          uint32_t& j) {
+  const uint32_t lead = __ldg(t.lead_base + t.n_clouds);
+  if (w < lead) {
+    cloud = find_cloud(t.lead_base, t.n_clouds, w);
+    j = w - __ldg(t.lead_base + cloud);
+    return;
+  }
+  // other tiles before cloud c: tile_base[c] - lead_base[c] (non-decreasing in c)
+  const uint32_t r = w - lead;
+  uint32_t lo = 0, hi = t.n_clouds;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(t.tile_base + mid) - __ldg(t.lead_base + mid) <= r) lo = mid; else hi = mid;
+  }
+  cloud = lo;
+  const uint32_t lead_c = __ldg(t.lead_base + lo + 1) - __ldg(t.lead_base + lo);
+  j = lead_c + (r - (__ldg(t.tile_base + lo) - __ldg(t.lead_base + lo)));
 }
 
 // Order-preserving map float -> uint32 (for atomicMin/Max on floats).

@@ -201,7 +201,7 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
   size_t off = 0;
   auto carve = [&](size_t bytes) { const size_t o = off; off += align256(bytes); return base + o; };
   Counters* ctr = (Counters*)carve(sizeof(Counters));
-  uint32_t* tables = (uint32_t*)carve(10 * 4);
+  uint32_t* tables = (uint32_t*)carve(12 * 4);
   CloudGrid* grids = (CloudGrid*)carve(sizeof(CloudGrid));
   uint32_t* bbox = (uint32_t*)carve(6 * 4);
   uint32_t* cells = (uint32_t*)carve((cap + 1) * 4);
@@ -230,6 +230,7 @@ extern "C" rtnn_status rtnn_search_noalloc(const float* d_points, uint32_t n_poi
   t.chunk_base = tables + 4;
   t.qchunk_base = tables + 6;
   t.tile_base = tables + 8;
+  t.lead_base = tables + 10;
   t.n_clouds = 1;
   const bool knn = mode == RTNN_MODE_KNN;
   bool in1 = false;

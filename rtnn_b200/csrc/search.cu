@@ -397,10 +397,10 @@ k_search(SearchArgs a) {
     uint32_t pos, cloud, entry;
     float wq = a.radius;
     if (main_pass) {
-      uint32_t c = 0;
-      if (lane == 0) c = find_cloud(a.t.tile_base, a.t.n_clouds, tile);
+      uint32_t c = 0, jt = 0;
+      if (lane == 0) main_tile(a.t, tile, c, jt);
       cloud = __shfl_sync(0xffffffffu, c, 0);
-      const uint32_t q0 = a.t.query_off[cloud] + (tile - a.t.tile_base[cloud]) * 32u;
+      const uint32_t q0 = a.t.query_off[cloud] + __shfl_sync(0xffffffffu, jt, 0) * 32u;
       pos = q0 + lane;
       entry = pos;
       valid = pos < a.t.query_off[cloud + 1];
@@ -1037,10 +1037,10 @@ k_search_q(SearchArgs a) {
     uint32_t pos, cloud, entry;
     float wq = a.radius;
     if (main_pass) {
-      uint32_t c = 0;
-      if (lane == 0) c = find_cloud(a.t.tile_base, a.t.n_clouds, tile);
+      uint32_t c = 0, jt = 0;
+      if (lane == 0) main_tile(a.t, tile, c, jt);
       cloud = __shfl_sync(0xffffffffu, c, 0);
-      pos = a.t.query_off[cloud] + (tile - a.t.tile_base[cloud]) * 32u + lane;
+      pos = a.t.query_off[cloud] + __shfl_sync(0xffffffffu, jt, 0) * 32u + lane;
       entry = pos;
       valid = pos < a.t.query_off[cloud + 1];
       if (valid && a.qwidth) wq = a.qwidth[pos];
