@@ -443,7 +443,9 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
     # the plain grid search (full radius for every query), with its own best tuning
     plain_tuning = at.autotune(ctx, *wl_args, knobs=at.GRID_KNOBS, presets=at.GRID_PRESETS,
                                use_cache=False, **common)
-    plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, **common)
+    # SPH time stepping: both paths keep the query order of their first execute across the
+    # steps (RTNN_FLAG_KEEP_ORDER; the grid is still rebuilt every step, rows stay exact)
+    plain = ctx.plan(cfg["offsets"], cfg["qoffsets"], use_graph=True, keep_order=sph, **common)
     # the headline times exactly `steps` steps; the other workloads time at least ~100 ms
     # per path (their steps take 0.2-50 ms), the same count for both paths
     if not headline:
@@ -460,7 +462,8 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
     learned_tuning, model_info = at.autotune_learned(
         ctx, *wl_args, train=lambda c: train_model(c, cfg, args.scale, rank),
         presets=at.GRID_PRESETS + [at.grid_of(plain_tuning)], **common)
-    learned = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=True, **common)
+    learned = ctx.plan(cfg["offsets"], cfg["qoffsets"], learned=True, use_graph=True,
+                       keep_order=sph, **common)
     ms_learned, clocks = timed(learned, steps, warmup, ClockSampler(dev) if headline else None)
     st = rtnn_b200.Stats()
     learned.execute(tp, tq, out, stats=st)
@@ -622,7 +625,10 @@ def run_rtnn(args, rank, world):
                 "best_value": world * oq / (best_ms * 1e-3),
                 "identical_sets": o["identical"], "fallback_queries": o["fallback"],
                 "config": {"mode": o["cfg"]["mode"], "radius": o["cfg"]["radius"], "k": o["K"],
-                           "n_points": o["N"], "n_queries": oq},
+                           "n_points": o["N"], "n_queries": oq,
+                           **({"time_stepping": "each step moves every particle by N(0, 0.05 h) "
+                               "and rebuilds the grid; the query order of the first step is "
+                               "kept (RTNN_FLAG_KEEP_ORDER)"} if name == "sph_lattice_5e7" else {})},
                 "stage_ms": o["stage_ms"], "roofline": {"frac": o["roofline"]["frac"],
                                                         "achieved": o["roofline"]["achieved"],
                                                         "unit": "GB/s", "kernel": "k_search (all passes)"},

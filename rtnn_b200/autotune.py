@@ -161,7 +161,8 @@ def autotune(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radi
 
 WIDTH_MODELS = [0, 1]   # rtnn_tuning.width_model: per query before the sort, per tile in the search
 OFF = 2                 # rtnn_tuning.width_model: learned widths switched off (full radius)
-MARGINS = [0.8, 0.9, 1.0, 1.1, 1.25]
+MARGINS = [0.9, 1.0, 1.08, 1.15, 1.25]
+CLIPS = [0, 4, 8]
 
 
 def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radius=0.2,
@@ -170,12 +171,12 @@ def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="kn
     on the kind of bucket, so for every cell-size preset and both kinds (width_model 0: a
     width per query before the sort; 1: a width per 32-query tile inside the search) the
     model is trained at that setting (`train(ctx)` collects training data and trains; what
-    it returns is handed back for the chosen setting) and the width margin is tuned; the
-    fastest setting keeps its model, then the search and learned knobs, which leave the
-    grid alone, are tuned by descent. Last, that setting is timed against the widths
-    switched off (width_model 2, the starting tuning: the plain search's) and the faster is
-    kept. Returns (tuning, train's result for the chosen setting plus "widths": "on" or
-    "off" and both times)."""
+    it returns is handed back for the chosen setting) and the width margin and the width
+    clip are tuned. The fastest setting keeps its model; then the search and learned knobs,
+    which leave the grid alone, are tuned by descent. Last, that setting is timed against
+    the widths switched off (width_model 2, the starting tuning: the plain search's) and the
+    faster is kept. Returns (tuning, train's result for the chosen setting plus "widths":
+    "on" or "off" and both times)."""
     import torch
     offsets = np.asarray(offsets, dtype=np.uint64)
     nq = int(offsets[-1]) if queries is None else int(np.asarray(qoffsets)[-1])
@@ -187,8 +188,11 @@ def autotune_learned(ctx, points, offsets, queries=None, qoffsets=None, mode="kn
         for kind in width_models if width_models is not None else WIDTH_MODELS:
             ctx.set_tuning(**{**start, **pre, "width_model": kind})
             info = train(ctx)
+            # the margin and the width clip interact (a clip trades box size for escalations),
+            # so both are tuned for every setting before the settings are compared
             tun = autotune(ctx, points, offsets, queries, qoffsets,
-                           knobs=[("width_margin", MARGINS)], use_cache=False, log=log, **kw)
+                           knobs=[("width_margin", MARGINS), ("width_clip", CLIPS)],
+                           use_cache=False, log=log, **kw)
             ms = time_plan(ctx, points, offsets, queries, qoffsets, out, **kw)
             if log:
                 log(f"autotune learned preset {pre} width_model {kind}: {ms:.3f} ms")
