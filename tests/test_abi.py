@@ -122,3 +122,30 @@ def test_headers_are_c99_and_link_from_c(tmp_path):
                     "-lrtnn_b200", "-Wl,-rpath," + lib_dir, "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, timeout=120)
     assert r.returncode in (0, 1)
+
+
+def test_python_structs_match_the_c_layout(tmp_path):
+    """The ctypes mirrors of rtnn_tuning and rtnn_stats have the C structs' sizes and field
+    offsets (a field added to the header without the Python mirror would shift every
+    later field)."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not found")
+    checks = []
+    for cname, py in (("rtnn_tuning", rtnn_b200.Tuning), ("rtnn_stats", rtnn_b200.Stats)):
+        checks.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            checks.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "rtnn.h"\n'
+                   "int main(void) {\n  " + "\n  ".join(checks) + "\n  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I" + os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out.splitlines()}
+    for cname, py in (("rtnn_tuning", rtnn_b200.Tuning), ("rtnn_stats", rtnn_b200.Stats)):
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
