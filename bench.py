@@ -450,7 +450,7 @@ def measure_workload(ctx, name, args, rank, world, dist, dev, steps, warmup, hea
     # per path (their steps take 0.2-50 ms), the same count for both paths
     if not headline:
         one, _ = timed(plain, 1, 1)
-        steps = int(min(200, max(steps, np.ceil(100.0 / max(one, 1e-3)))))
+        steps = int(min(1000, max(steps, np.ceil(100.0 / max(one, 1e-3)))))
     plain_ms, _ = timed(plain, steps, warmup)
 
     # learned partition: starting from the plain search's tuned settings, for each

@@ -14,9 +14,9 @@
 //      row costs two offset loads (computed lane-parallel, 32 rows at a time); rows, and
 //      the ends of rows, farther than R from the bbox are skipped (RowClip);
 //   3. 32 rows at a time are streamed as one flattened candidate sequence with 16-byte
-//      loads (rows in a stride-permuted order), the points farther than R from the tile
-//      box are dropped, and the survivors are compacted with __ballot_sync into a
-//      per-warp shared-memory stage;
+//      loads issued one batch of 32 ahead (rows in a stride-permuted order), the points
+//      farther than R from the tile box are dropped, and the survivors are compacted with
+//      __ballot_sync into a per-warp shared-memory stage;
 //   4. every lane tests every staged point against its own query with the reference's
 //      FP32 distance (common.cuh: dist2_ref) and keeps its K smallest (distance, index)
 //      pairs in a per-lane column in shared memory ([slot][lane], conflict-free): hits are
@@ -725,21 +725,35 @@ k_search(SearchArgs a) {
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         const uint32_t shift = rs - (incl - len);   // candidate t of this row: spts[t + shift]
-        for (uint32_t b = 0; b < total; b += 32) {
-          // 3. stream 32 candidates, drop those farther than R from the box, compact the
-          //    survivors behind the ones already staged (rows accumulate)
-          const uint32_t t = b + lane;
-          int row = 0;   // rows whose end is <= t (binary search over the lanes' ends)
+        // index in spts of candidate t: rows whose end is <= t (binary search over the
+        // lanes' scanned ends), then that row's shift
+        auto cand = [&](uint32_t t) -> uint32_t {
+          int row = 0;
 #pragma unroll
           for (int step = 16; step > 0; step >>= 1) {
             const uint32_t e = __shfl_sync(0xffffffffu, incl, row + step - 1);
             if (e <= t) row += step;
           }
-          const uint32_t idx = t + __shfl_sync(0xffffffffu, shift, row);
+          return t + __shfl_sync(0xffffffffu, shift, row);
+        };
+        // the loads run one batch ahead: the next 32 candidates are in flight while this
+        // batch is filtered, compacted and (once 32 are staged) tested
+        float4 pn = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (total > 0) {
+          const uint32_t idx0 = cand(lane);
+          if (lane < total) pn = __ldg(a.spts + idx0);
+        }
+        for (uint32_t b = 0; b < total; b += 32) {
+          // 3. stream 32 candidates, drop those farther than R from the box, compact the
+          //    survivors behind the ones already staged (rows accumulate)
+          const uint32_t t = b + lane;
+          const float4 p = pn;
+          if (b + 32 < total) {
+            const uint32_t idxn = cand(t + 32);
+            if (t + 32 < total) pn = __ldg(a.spts + idxn);
+          }
           bool keep = false;
-          float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
           if (t < total) {
-            p = __ldg(a.spts + idx);
             const float ex = fmaxf(fmaxf(bx0 - p.x, p.x - bx1), 0.f);
             const float ey = fmaxf(fmaxf(by0 - p.y, p.y - by1), 0.f);
             const float ez = fmaxf(fmaxf(bz0 - p.z, p.z - bz1), 0.f);
