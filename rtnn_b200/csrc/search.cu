@@ -28,6 +28,7 @@
 // and the last pass at the full radius, so every row is exact.
 #include "common.cuh"
 #include "kernels.h"
+#include "packed.cuh"
 #include "tile_model.cuh"
 
 namespace rtnn {
@@ -87,46 +88,6 @@ __device__ __forceinline__ void heapify_fixed(uint64_t* h) {
     heap_sift_fixed<K, I>(h, h[I * 32]);
     heapify_fixed<K, I - 1>(h);
   }
-}
-
-// ---- packed FP32x2 arithmetic (sm_100a): two IEEE round-to-nearest operations per
-//      instruction, each element rounded on its own exactly like __fsub_rn / __fmul_rn /
-//      __fadd_rn, so two candidates' distances cost one instruction chain
-__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
-  uint64_t r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void upk2(uint64_t v, uint32_t& lo, uint32_t& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(v));
-}
-__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-// dist2_ref of two points at once: ((dx*dx + dy*dy) + dz*dz), every step rounded.
-// Differences and squares are packed; the two sums are scalar __fadd_rn. A packed add
-// whose second operand is a packed product was measured to be fused into a single-rounding
-// multiply-add by the compiler even with .rn (about 12 % of results off by an ulp), which
-// would break the bit-exact distances; scalar adds after packed products matched scalar
-// arithmetic bit for bit on 2^20 random pairs.
-__device__ __forceinline__ void dist2_pair(uint64_t qx, uint64_t qy, uint64_t qz, uint64_t px,
-                                           uint64_t py, uint64_t pz, uint32_t& d0, uint32_t& d1) {
-  const uint64_t dx = sub2(qx, px), dy = sub2(qy, py), dz = sub2(qz, pz);
-  uint32_t x0, x1, y0, y1, z0, z1;
-  upk2(mul2(dx, dx), x0, x1);
-  upk2(mul2(dy, dy), y0, y1);
-  upk2(mul2(dz, dz), z0, z1);
-  d0 = __float_as_uint(__fadd_rn(__fadd_rn(__uint_as_float(x0), __uint_as_float(y0)),
-                                 __uint_as_float(z0)));
-  d1 = __float_as_uint(__fadd_rn(__fadd_rn(__uint_as_float(x1), __uint_as_float(y1)),
-                                 __uint_as_float(z1)));
 }
 
 // Staged candidates are kept in pairs, {x0 x1 y0 y1 | z0 z1 w0 w1} (32 bytes per two
@@ -1114,6 +1075,7 @@ k_search_q(SearchArgs a) {
 
       uint32_t wlo, wspan;   // hit window on the distance bits (see hit_window)
       hit_window(true, limj, INFINITY, KNN, wlo, wspan);
+      const uint64_t qx2 = pk2(qx, qx), qy2 = pk2(qy, qy), qz2 = pk2(qz, qz);
       uint32_t nb = 0;       // hits in the buffer (warp-uniform)
       bool stop = false;     // any_k: k hits found
       const RowSplit split(ny > 0 ? (uint32_t)ny : 1u, (uint32_t)nrows);
@@ -1138,8 +1100,8 @@ k_search_q(SearchArgs a) {
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         const uint32_t shift = rs - (incl - len);   // candidate t of this row: spts[t + shift]
-        // two candidates per lane per step (t and t + 32): independent lookups, loads and
-        // distances for the latency to overlap
+        // two candidates per lane per step (t and t + 32): independent lookups and loads
+        // for the latency to overlap, and one packed distance chain for the pair
         for (uint32_t b = 0; b < total; b += 64) {
           const uint32_t t0 = b + lane, t1 = b + 32 + lane;
           int r0 = 0, r1 = 0;
@@ -1156,15 +1118,13 @@ k_search_q(SearchArgs a) {
           uint64_t key0 = 0, key1 = 0;
           const float4 p0 = t0 < total ? __ldg(a.spts + idx0) : make_float4(0.f, 0.f, 0.f, 0.f);
           const float4 p1 = t1 < total ? __ldg(a.spts + idx1) : make_float4(0.f, 0.f, 0.f, 0.f);
-          if (t0 < total) {
-            const uint32_t d = __float_as_uint(dist2_ref(qx, qy, qz, p0.x, p0.y, p0.z));
-            hit0 = d - wlo <= wspan;
-            key0 = ((uint64_t)d << 32) | __float_as_uint(p0.w);
-          }
-          if (t1 < total) {
-            const uint32_t d = __float_as_uint(dist2_ref(qx, qy, qz, p1.x, p1.y, p1.z));
-            hit1 = d - wlo <= wspan;
-            key1 = ((uint64_t)d << 32) | __float_as_uint(p1.w);
+          {
+            uint32_t d0, d1;
+            dist2_pair(qx2, qy2, qz2, pk2(p0.x, p1.x), pk2(p0.y, p1.y), pk2(p0.z, p1.z), d0, d1);
+            hit0 = t0 < total && d0 - wlo <= wspan;
+            hit1 = t1 < total && d1 - wlo <= wspan;
+            key0 = ((uint64_t)d0 << 32) | __float_as_uint(p0.w);
+            key1 = ((uint64_t)d1 << 32) | __float_as_uint(p1.w);
           }
           const uint32_t m0 = __ballot_sync(0xffffffffu, hit0);
           const uint32_t m1 = __ballot_sync(0xffffffffu, hit1);
