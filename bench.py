@@ -132,7 +132,7 @@ def run_profile(args):
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     # the tuning the autotuner settles on for the default workload: fine cells, tiles for
     # the first pass and one warp per query for the escalation passes
-    ctx.set_tuning(points_per_cell=0.125, cell_ratio=0.125, min_cell_ratio=0.01, width_margin=1.08,
+    ctx.set_tuning(points_per_cell=0.125, cell_ratio=0.125, min_cell_ratio=0.01, width_margin=1.1,
                    fallback_passes=4, gap_ratio=2.0, pending_slots=16, query_warps=2,
                    buckets_per_halving=1.0, width_model=args.width_model, width_clip=8)
     learned = args.profile_path == "learned"

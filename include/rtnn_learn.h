@@ -4,7 +4,7 @@
  * The reference picks each partition's launch radius with an analytic rule: grow a box
  * of cells until it holds K+1 points (calcSearchSize, src/optixNSearch/grid.cu:84-211)
  * and take the equal-volume sphere radius of that box (radiusFromMegacell,
- * sort.cpp:262-269; autoBatchingKNN, sort.cpp:271-320). Here a small MLP (6 -> 32 -> 32
+ * sort.cpp:262-269; autoBatchingKNN, sort.cpp:271-320). Here a small MLP (6 -> 16 -> 16
  * -> 1, ReLU) predicts a bucket's search width from its occupancy histogram (log1p of the
  * points in cell shells 0, 1, 2, and log(K+1) - log1p(N2)), log(cell / r) and its extent.
  * Two kinds of bucket, chosen by rtnn_tuning.width_model:
@@ -22,7 +22,7 @@
  * The network is trained on the GPU by hand-written kernels (forward, backward, Adam)
  * on exact K-th distances produced by the plain search. All pointers are device
  * pointers. Parameters: rtnn_model_size() floats laid out as
- *   in_mean[6] in_std[6] out_mean out_std | W1[32][6] b1[32] W2[32][32] b2[32] W3[32] b3
+ *   in_mean[6] in_std[6] out_mean out_std | W1[16][6] b1[16] W2[16][16] b2[16] W3[16] b3
  * (gradients cover the part after '|': rtnn_model_size() - 14 floats).
  */
 #ifndef RTNN_LEARN_H_
@@ -35,6 +35,7 @@ extern "C" {
 #endif
 
 #define RTNN_MODEL_FEATURES 6
+#define RTNN_MODEL_HIDDEN 16
 #define RTNN_MODEL_NORM_PARAMS 14
 
 uint32_t rtnn_model_size(void);

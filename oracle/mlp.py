@@ -1,14 +1,14 @@
 """FP64 numpy restatement of the width MLP -- TEST INFRASTRUCTURE ONLY.
 
 Checks the hand-written CUDA forward / backward / Adam kernels of the learned
-partition (6 -> 32 -> 32 -> 1, ReLU; parameter layout of include/rtnn_learn.h). The
+partition (6 -> 16 -> 16 -> 1, ReLU; parameter layout of include/rtnn_learn.h). The
 reference has no learned model (its widths come from calcSearchSize, grid.cu:84-211), so
 this restatement is pinned against finite differences instead of reference outputs.
 """
 import numpy as np
 
 F = 6
-H = 32
+H = 16
 NORM = 2 * F + 2
 
 

@@ -31,6 +31,7 @@ FLAG_KEEP_ORDER = 0x40
 FLAG_REF_LAYOUT = 0x80
 MAX_K = 128
 MODEL_FEATURES = 6   # RTNN_MODEL_FEATURES
+MODEL_HIDDEN = 16    # RTNN_MODEL_HIDDEN
 MODEL_NORM_PARAMS = 2 * MODEL_FEATURES + 2   # RTNN_MODEL_NORM_PARAMS
 
 _STATUS = {

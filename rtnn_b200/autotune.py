@@ -49,7 +49,7 @@ GRID_PRESETS = [
 # the learned widths are per tile (the search's bucket), so the analytic partition's
 # width buckets (buckets_per_halving) do not apply
 LEARNED_KNOBS = [
-    ("width_margin", [0.8, 0.9, 1.0, 1.08, 1.15, 1.25]),
+    ("width_margin", [0.8, 0.9, 1.0, 1.05, 1.1, 1.15, 1.25]),
     ("fallback_passes", [2, 4, 6]),
     ("width_clip", [0, 2, 4, 8]),
 ]
@@ -161,7 +161,7 @@ def autotune(ctx, points, offsets, queries=None, qoffsets=None, mode="knn", radi
 
 WIDTH_MODELS = [0, 1]   # rtnn_tuning.width_model: per query before the sort, per tile in the search
 OFF = 2                 # rtnn_tuning.width_model: learned widths switched off (full radius)
-MARGINS = [0.9, 1.0, 1.08, 1.15, 1.25]
+MARGINS = [0.9, 1.0, 1.05, 1.1, 1.15, 1.25]
 CLIPS = [0, 4, 8]
 
 

@@ -125,7 +125,7 @@ cudaError_t launch_compact_fallback(const uint32_t* flags, uint32_t n_host, cons
 // partition.cu -- density buckets: per-query search widths (analytic or learned MLP)
 constexpr int kShells = 3;                 // box counts N_0..N_2 around a query's cell
 constexpr int kFeatDim = 6;                // MLP input features per query
-constexpr int kHidden = 32;                // MLP hidden width (two hidden layers)
+constexpr int kHidden = 16;                // MLP hidden width (two hidden layers)
 // parameter layout (floats): in_mean[F] in_std[F] out_mean out_std | W1[H][F] b1[H]
 // W2[H][H] b2[H] W3[H] b3  -- only the part after '|' is trained
 constexpr int kNormParams = 2 * kFeatDim + 2;

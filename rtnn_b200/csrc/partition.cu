@@ -25,7 +25,7 @@
 namespace rtnn {
 namespace {
 
-// ---- MLP (6 -> 32 -> 32 -> 1, ReLU) ------------------------------------------------
+// ---- MLP (6 -> 16 -> 16 -> 1, ReLU) ------------------------------------------------
 static_assert(kFeatDim == kTileFeat && kHidden == kTileHidden,
               "the trained MLP is the one the search evaluates");
 

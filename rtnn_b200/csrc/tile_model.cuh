@@ -5,7 +5,7 @@
 // each occupied cell grows a box of cells until it holds K + 1 points and its queries are
 // launched with the equal-volume radius of that box. Here the bucket is the tile of 32
 // consecutive queries (Hilbert order) that one warp of the search handles, and a small MLP
-// (6 -> 32 -> 32 -> 1, ReLU) reads the bucket's features
+// (6 -> 16 -> 16 -> 1, ReLU) reads the bucket's features
 //   f0..f2  log1p of the points in cell shells 0, 1, 2 around the cell of the tile's
 //           bounding-box centre (the occupancy histogram: N0, N1 - N0, N2 - N1),
 //   f3      log(K + 1) - log1p(N2),
@@ -24,8 +24,9 @@
 namespace rtnn {
 
 constexpr int kTileFeat = 6;       // MLP input features per tile
-constexpr int kTileHidden = 32;    // hidden units: one per lane
-static_assert(kTileHidden == 32, "the warp-collective MLP gives every lane one hidden unit");
+constexpr int kTileHidden = 16;    // hidden units: lanes j and j + 16 compute unit j
+static_assert(32 % kTileHidden == 0 && kTileHidden % 4 == 0,
+              "the warp-collective MLP spreads the hidden units over the lanes");
 
 __device__ __forceinline__ float warp_sum_f(float v) {
 #pragma unroll
@@ -79,18 +80,20 @@ __device__ __forceinline__ void tile_features(const CloudGrid& g, const uint32_t
 }
 
 // The model's prediction (denormalised: log(K-th distance / cell)) for one feature vector.
-// Parameter layout (floats): in_mean[6] in_std[6] out_mean out_std | W1[32][6] b1[32]
-// W2[32][32] b2[32] W3[32] b3, P at least 8-byte aligned (a device allocation is). Lane j
-// computes hidden unit j of both layers; the first layer's units reach every lane through
-// `scratch` (32 floats of this warp's shared memory, 16-byte aligned), read back as eight
+// Parameter layout (floats): in_mean[6] in_std[6] out_mean out_std | W1[H][6] b1[H]
+// W2[H][H] b2[H] W3[H] b3 (H = kTileHidden), P at least 8-byte aligned (a device allocation
+// is). Lane j computes hidden unit j mod H of both layers (the lanes past H repeat the
+// first H and add nothing to the output); the first layer's units reach every lane through
+// `scratch` (32 floats of this warp's shared memory, 16-byte aligned), read back as H / 4
 // broadcast 16-byte loads, and the second layer sums in four independent chains, so the
-// evaluation is a few short dependency chains instead of 32 shuffles in a row; the output is
-// a warp sum. (The sums run in another order than the inference kernel's: the two agree to
+// evaluation is a few short dependency chains instead of H shuffles in a row; the output
+// is a warp sum. (The sums run in another order than the inference kernel's: the two agree to
 // FP32 rounding, which only moves a search width, never a result.)
 __device__ __forceinline__ float tile_mlp(const float* __restrict__ P, const float* feat,
                                           float* scratch) {
   constexpr int F = kTileFeat, H = kTileHidden;
-  const int j = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
+  const int j = lane & (H - 1);
   const float* W1 = P + 2 * F + 2;
   const float* b1 = W1 + H * F;
   const float* W2 = b1 + H;
@@ -103,9 +106,10 @@ __device__ __forceinline__ float tile_mlp(const float* __restrict__ P, const flo
 #pragma unroll
   for (int f = 0; f < F; ++f) h1 = fmaf(__ldg(W1 + j * F + f), xn[f], h1);
   __syncwarp();
-  scratch[j] = fmaxf(h1, 0.f);
+  if (lane < H) scratch[j] = fmaxf(h1, 0.f);
   __syncwarp();
-  // W2 starts 238 floats into P: 8-byte aligned (P itself is 256-byte aligned), not 16
+  // W2 starts 2 F + 2 + H (F + 1) floats into P (126): 8-byte aligned (P itself is
+  // 256-byte aligned), not 16
   const float2* w2 = reinterpret_cast<const float2*>(W2 + j * H);
   const float4* hv = reinterpret_cast<const float4*>(scratch);
   float acc[4] = {__ldg(b2 + j), 0.f, 0.f, 0.f};
@@ -120,7 +124,7 @@ __device__ __forceinline__ float tile_mlp(const float* __restrict__ P, const flo
   }
   __syncwarp();
   const float h2 = fmaxf((acc[0] + acc[1]) + (acc[2] + acc[3]), 0.f);
-  const float o = warp_sum_f(__ldg(W3 + j) * h2) + __ldg(W3 + H);
+  const float o = warp_sum_f(lane < H ? __ldg(W3 + j) * h2 : 0.f) + __ldg(W3 + H);
   return fmaf(o, __ldg(P + 2 * F + 1), __ldg(P + 2 * F));
 }
 

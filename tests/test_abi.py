@@ -48,7 +48,7 @@ def test_version_and_k_range():
 
 def test_model_size_matches_layout():
     lib = rtnn_b200.load_library()
-    F, H = 6, 32
+    F, H = rtnn_b200.MODEL_FEATURES, rtnn_b200.MODEL_HIDDEN
     assert lib.rtnn_model_size() == 2 * F + 2 + H * F + H + H * H + H + H + 1
 
 
@@ -56,7 +56,11 @@ def test_python_model_constants_match_header():
     hdr = open(os.path.join(ROOT, "include", "rtnn_learn.h")).read()
     feats = int(re.search(r"#define RTNN_MODEL_FEATURES (\d+)", hdr).group(1))
     norm = int(re.search(r"#define RTNN_MODEL_NORM_PARAMS (\d+)", hdr).group(1))
+    hidden = int(re.search(r"#define RTNN_MODEL_HIDDEN (\d+)", hdr).group(1))
     assert (feats, norm) == (rtnn_b200.MODEL_FEATURES, rtnn_b200.MODEL_NORM_PARAMS)
+    assert hidden == rtnn_b200.MODEL_HIDDEN
+    from oracle import mlp
+    assert (mlp.F, mlp.H, mlp.NORM) == (feats, hidden, norm)
     assert norm == 2 * feats + 2
 
 
