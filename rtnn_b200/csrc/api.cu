@@ -233,7 +233,7 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
   uint32_t* qb = cb + n1;
   uint32_t* tb = qb + n1;
   uint32_t* lb = tb + n1;
-  uint64_t chunks = 0, qchunks = 0, tiles = 0, leads = 0, maxq = 0;
+  uint64_t chunks = 0, qchunks = 0, tiles = 0, maxq = 0;
   for (uint32_t i = 0; i < n_clouds; ++i) {
     if (point_off[i + 1] < point_off[i] || qoff[i + 1] < qoff[i])
       return fail(c, RTNN_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
@@ -243,11 +243,9 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
     cb[i] = (uint32_t)chunks;
     qb[i] = (uint32_t)qchunks;
     tb[i] = (uint32_t)tiles;
-    lb[i] = (uint32_t)leads;
     chunks += (np + kChunk - 1) / kChunk;
     qchunks += (nq + kChunk - 1) / kChunk;
     tiles += (nq + kTile - 1) / kTile;
-    leads += lead_tiles((uint32_t)((nq + kTile - 1) / kTile));
     maxq = std::max(maxq, nq);
   }
   sh.N = point_off[n_clouds];
@@ -259,6 +257,16 @@ rtnn_status batched_shapes(rtnn_ctx* c, const uint64_t* point_off, uint32_t n_cl
   cb[n_clouds] = (uint32_t)chunks;
   qb[n_clouds] = (uint32_t)qchunks;
   tb[n_clouds] = (uint32_t)tiles;
+  // lead tiles (common.cuh: main_tile) only for the clouds whose tiles start in the last
+  // eighth of the pass: their long tiles would otherwise start near its end. The other
+  // clouds keep plain cloud order (their widest tiles lead each cloud anyway), so that a
+  // cloud's tiles run close together in time and share its candidates in L2.
+  const uint64_t tail_from = tiles - (tiles >> kLeadShift);
+  uint64_t leads = 0;
+  for (uint32_t i = 0; i < n_clouds; ++i) {
+    lb[i] = (uint32_t)leads;
+    if (tb[i] >= tail_from) leads += lead_tiles(tb[i + 1] - tb[i]);
+  }
   lb[n_clouds] = (uint32_t)leads;
   sh.n_chunks = (uint32_t)chunks;
   sh.n_qchunks = (uint32_t)qchunks;

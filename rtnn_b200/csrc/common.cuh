@@ -73,8 +73,10 @@ struct CloudTables {
 // The lead tiles of a cloud are the first eighth of its tiles (rounded up): the queries
 // are sorted widest width bucket first, so they hold the cloud's widest searches -- the
 // longest tiles by far (up to a few ms where a wide box reaches a dense blob). The first
-// search pass takes the lead tiles of every cloud before any other tile, so that no long
-// tile starts near the end of the pass and holds it while the other SMs are idle.
+// search pass takes the lead tiles of the clouds at the end of the pass (lead_base counts
+// them; the host gives lead tiles to the clouds whose tiles start in the last eighth)
+// before any other tile, so that no long tile starts near the end of the pass and holds it
+// while the other SMs are idle.
 constexpr uint32_t kLeadShift = 3;
 __host__ __device__ __forceinline__ uint32_t lead_tiles(uint32_t tiles) {
   return (tiles + (1u << kLeadShift) - 1u) >> kLeadShift;
