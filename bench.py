@@ -35,14 +35,14 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per query of the main search pass, from the ncu capture in
-# profiles/kernels_knn_multicloud_scale0.3.md (3,528 MB for 16.28 M queries), scaled by
+# profiles/kernels_knn_multicloud_scale0.3.md (3,646 MB for 16.28 M queries), scaled by
 # queries to a full launch; only known for the default workload.
-TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 216.8}
+TRAFFIC_PER_QUERY = {"knn_multicloud_4096": 224.0}
 # Warp instructions per query of the first search pass (smsp__inst_executed.sum over the
 # queries in the capture of profiles/k_search_knn_multicloud_scale0.1.md with K = 32
-# compiled in and the widths clipped: 4.036e9 for 5.25 M queries). The search is bound by
+# compiled in and the widths clipped: 4.223e9 for 5.25 M queries). The search is bound by
 # instruction issue, not DRAM, so the bench also reports the issue rate this implies.
-INST_PER_QUERY = {"knn_multicloud_4096": 768.7}
+INST_PER_QUERY = {"knn_multicloud_4096": 804.3}
 # Per-kernel ncu figures of one learned step plus one width-model training step of the
 # default workload at scale 0.3 (1,228 clouds, 16,276,803 points = queries), from the
 # capture summarised in profiles/kernels_knn_multicloud_scale0.3.md (gpu__time_duration.sum,
@@ -50,23 +50,23 @@ INST_PER_QUERY = {"knn_multicloud_4096": 768.7}
 # kernel -> (launches, total us, DRAM bytes, algorithmic bytes per unit, unit); 0 where the
 # kernel's work is not counted in bytes (per short query, or training samples).
 KERNEL_PROFILE = {"knn_multicloud_4096": {"units": 16276803, "kernels": {
-        "k_bbox": (1, 91.2, 198973184, 12, "point"),
-        "k_grid_plan": (1, 11.1, 49664, 0, "point"),
-        "k_zero_cells": (1, 93.6, 498732544, 34, "point"),
-        "k_count": (1, 213.2, 477521152, 16, "point"),
-        "k_scan_excl": (11, 568.7, 1191682304, 68.8, "point"),
-        "k_scatter": (1, 194.2, 688746752, 36, "point"),
-        "k_widths": (1, 1851.4, 753006848, 20, "query"),
-        "k_query_keys<unsigned long>": (1, 276.6, 358198528, 20, "query"),
-        "k_radix_hist<unsigned long>": (5, 253.7, 663625984, 40, "query"),
-        "k_radix_scatter<unsigned long>": (5, 729.7, 1683483392, 116, "query"),
-        "k_gather_queries": (1, 202.5, 661687296, 32, "query"),
-        "k_search<1, 32, 0>": (1, 18629.6, 3528351232, 160, "query"),
-        "k_compact_fallback": (5, 147.5, 145904384, 8, "query"),
-        "k_search_q<1, 32>": (5, 5432.9, 1797241856, 0, "query"),
-        "k_mlp_loss_grad": (1, 215.3, 836096, 0, "sample"),
-        "k_mlp_adam": (1, 5.8, 29952, 0, "sample"),
-        "k_mlp_forward": (1, 11.8, 306176, 0, "sample"),
+        "k_bbox": (1, 90.8, 199129600, 12, "point"),
+        "k_grid_plan": (1, 11.2, 49664, 0, "point"),
+        "k_zero_cells": (1, 93.8, 498550272, 34, "point"),
+        "k_count": (1, 213.7, 477383936, 16, "point"),
+        "k_scan_excl": (11, 588.6, 1188800512, 68.8, "point"),
+        "k_scatter": (1, 194.8, 687007232, 36, "point"),
+        "k_widths": (1, 932.9, 921034240, 20, "query"),
+        "k_query_keys<unsigned long>": (1, 276.8, 358948864, 20, "query"),
+        "k_radix_hist<unsigned long>": (5, 252.6, 664852992, 40, "query"),
+        "k_radix_scatter<unsigned long>": (5, 723.3, 1680649472, 116, "query"),
+        "k_gather_queries": (1, 202.0, 663449088, 32, "query"),
+        "k_search<1, 32, 0>": (1, 18535.9, 3646300416, 160, "query"),
+        "k_compact_fallback": (5, 138.0, 134351104, 8, "query"),
+        "k_search_q<1, 32>": (5, 4459.9, 1982381568, 0, "query"),
+        "k_mlp_loss_grad": (1, 67.2, 492288, 0, "sample"),
+        "k_mlp_adam": (1, 5.6, 15104, 0, "sample"),
+        "k_mlp_forward": (1, 7.3, 299776, 0, "sample"),
 }}}
 
 
